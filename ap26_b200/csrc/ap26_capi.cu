@@ -1,0 +1,961 @@
+// ap26_capi.cu -- C ABI of libap26.so: context, per-K search, batched
+// persistent search, serving loop, kernel-level entry points.
+//
+// Replaces the reference's GPU host orchestration (ibethune/ap26,
+// src/opencl/AP26.h:78-346 SearchAP26, src/common/AP26.cpp:834-939 set-up):
+// one H2D of the K-job descriptors, a chunked chain of kernels on one
+// stream (optionally replayed from a CUDA graph), one D2H of the raw reports.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/ap26.h"
+#include "ap26_kernels.cuh"
+#include "ap26_hostcore.h"
+
+namespace ap26 {
+
+// ---- per-job set-up kernel ----------------------------------------------------
+// Thread 0: the reference's per-K constants (src/opencl/AP26.h:112-120, int64
+// split multiplications).  All threads: the bitstrings
+//   B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
+// OK_p[r] = 0 iff r = (jj * (STEP mod p)) mod p for some jj in [p-23, p]
+// (MAKE_OK, src/cpu/cpusse2.cpp:32-36; setok.cl:79-81).
+__device__ int kmul_mod(int64_t c, int K, int64_t *out) {
+  *out = (c * (K % 17835) + ((c * 17835) % MOD) * (K / 17835)) % MOD;
+  return 0;
+}
+
+__global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables) {
+  const int j = blockIdx.x;
+  if (j >= njobs) return;
+  KJob &J = jobs[j];
+  const int K = J.K, shift = J.shift;
+  if (threadIdx.x == 0) {
+    J.STEP = (int64_t)K * PRIM23;
+    J.n0 = (N0 * (K % 17835) + ((N0 * 17835) % MOD) * (K / 17835) + N30) % MOD;
+    kmul_mod(PRES2, K, &J.S31);
+    kmul_mod(PRES3, K, &J.S37);
+    kmul_mod(PRES4, K, &J.S41);
+    kmul_mod(PRES5, K, &J.S43);
+    kmul_mod(PRES6, K, &J.S47);
+    kmul_mod(PRES7, K, &J.S53);
+    kmul_mod(PRES8, K, &J.S59);
+  }
+  uint32_t *tab = tables + (size_t)j * TABLE_WORDS;
+  for (int t = threadIdx.x; t < TABLE_WORDS; t += blockDim.x) {
+    int g = 0;
+    while (g + 1 < NPRIMES && c_params[g + 1].off <= t) g++;
+    const int p = c_params[g].p;
+    const int st = (int)(((int64_t)(K % p) * (int)(PRIM23 % p)) % p);
+    int stinv = 0;
+    if (st) {  // st^(p-2) mod p
+      int e = p - 2, base = st, r = 1;
+      while (e) { if (e & 1) r = r * base % p; base = base * base % p; e >>= 1; }
+      stinv = r;
+    }
+    const int cm = (int)(MOD % p);
+    const int sh = shift % p;
+    const int j0 = (t - c_params[g].off) * 32;
+    uint32_t word = 0;
+    for (int u = 0; u < 32; u++) {
+      const int x = (j0 + u + sh) % p;
+      const int r = x * cm % p;
+      bool bad;
+      if (st == 0) bad = (r == 0);
+      else { const int tt = r * stinv % p; bad = (tt == 0) || (tt >= p - 23); }
+      if (!bad) word |= 1u << u;
+    }
+    tab[t] = word;
+  }
+}
+
+__global__ void chunk_begin_kernel(DevState *st) {
+  st->tile_next = st->chunk_begin;
+  unsigned long long e = st->chunk_begin + st->chunk_size;
+  st->tile_end = e < st->total_tiles ? e : st->total_tiles;
+  st->cand_count = 0;
+}
+
+__global__ void chunk_end_kernel(DevState *st, long long cand_cap) {
+  unsigned long long c = st->cand_count;
+  st->cand_total += c;
+  if ((long long)c > cand_cap) st->err_flags |= ERR_CAND_OVERFLOW;
+  st->chunk_begin += st->chunk_size;
+}
+
+// ---- peak probes: conflict-free LDS.128 stream and dependent-free IMAD chains ----
+__global__ void smem_probe_kernel(int iters, unsigned *sink) {
+  __shared__ uint4 buf[1024];
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) buf[i] = make_uint4(i, i * 3, i * 5, i * 7);
+  __syncthreads();
+  uint4 acc = make_uint4(0, 0, 0, 0);
+  int idx = threadIdx.x & 1023;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      uint4 v = buf[(idx + u * 128) & 1023];
+      acc.x ^= v.x; acc.y ^= v.y; acc.z ^= v.z; acc.w ^= v.w;
+    }
+    idx = (idx + 32) & 1023;
+  }
+  if ((acc.x ^ acc.y ^ acc.z ^ acc.w) == 0x12345678u) sink[0] = 1;
+}
+
+__global__ void int_probe_kernel(int iters, unsigned *sink) {
+  uint32_t a0 = threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5,
+           a6 = a0 + 6, a7 = a0 + 7;
+  const uint32_t m = 0x9E3779B1u, c = blockIdx.x | 1;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      a0 = a0 * m + c; a1 = a1 * m + c; a2 = a2 * m + c; a3 = a3 * m + c;
+      a4 = a4 * m + c; a5 = a5 * m + c; a6 = a6 * m + c; a7 = a7 * m + c;
+    }
+  }
+  if ((a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7) == 0x12345678u) sink[0] = 1;
+}
+
+// ---- PRP microbenchmark kernel: verdicts of sprp2 over an array ----------------
+__global__ void sprp_batch_kernel(const uint64_t *N, long long count, uint8_t *verdict,
+                                  unsigned long long *squarings) {
+  unsigned sq = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    const uint64_t n = N[i];
+    verdict[i] = (uint8_t)((n & 1) && n < (1ull << 63) ? sprp2(n, sq) : 0);
+  }
+  unsigned v = sq;
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(squarings, (unsigned long long)v);
+}
+
+// Chain walk for explicit candidates (kernel-level parity entry point).
+__global__ void chain_explicit_kernel(const KJob *job, const int64_t *n, long long count,
+                                      int32_t *k_out, int64_t *first_out, DevState *st) {
+  unsigned tests = 0, sq = 0;
+  const int64_t S = job->STEP;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    int k = 0;
+    int64_t m = n[i] + S * 5;
+    while (prp_term(st, m, tests, sq)) { k++; m += S; }
+    if (k >= 10) {
+      m = n[i] + S * 4;
+      while (m > 0 && prp_term(st, m, tests, sq)) { k++; m -= S; }
+    }
+    k_out[i] = k;
+    first_out[i] = m + S;
+  }
+}
+
+// ---- sieve variants (autotuner candidates) --------------------------------------
+struct SieveVariant {
+  int G, R, SL, QCAP, WARPS;
+  void (*kernel)(SieveArgs);
+  size_t smem() const { return sizeof(uint4) * QCAP * WARPS + sizeof(uint32_t) * TABLE_WORDS; }
+};
+
+#define AP26_VARIANT(G, R, SL, Q, W) \
+  SieveVariant{G, R, SL, Q, W, sieve_kernel<G, R, SL, Q, W>}
+
+static const SieveVariant kVariants[] = {
+    AP26_VARIANT(16, 4, 44, 448, 8),   // default
+    AP26_VARIANT(12, 4, 44, 448, 8),
+    AP26_VARIANT(20, 4, 44, 448, 8),
+    AP26_VARIANT(16, 4, 44, 640, 4),
+    AP26_VARIANT(16, 4, 36, 448, 8),
+    AP26_VARIANT(16, 4, 52, 448, 8),
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+}  // namespace ap26
+
+using namespace ap26;
+
+// ---- context --------------------------------------------------------------------
+struct ServeUnit {
+  ap26_item item;
+  std::vector<int> ks;           // searchable K of the unit
+  size_t next_k = 0;             // next K to put on the device
+  int inflight = 0;              // K-jobs of this unit in the current slice
+  int done_k = 0;
+  std::vector<ap26_ap> aps;
+  int64_t candidates = 0;
+  int status = AP26_OK;
+  std::chrono::steady_clock::time_point t_submit;
+  double latency_ms = 0;
+};
+
+struct ap26_ctx {
+  int device = 0;
+  ap26_opts opts{};
+  int variant = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int num_sms = 0, sieve_blocks = 0, chain_blocks = 0;
+  // device buffers
+  KJob *d_jobs = nullptr;
+  uint32_t *d_tables = nullptr;
+  unsigned long long *d_job_counts = nullptr;
+  int jobs_cap = 0;
+  DevState *d_st = nullptr;
+  Cand *d_cand = nullptr;
+  long long cand_cap = 0;
+  APRec *d_aps = nullptr;
+  long long ap_cap = 0;
+  // pinned host mirrors
+  KJob *h_jobs = nullptr;
+  DevState *h_st = nullptr;
+  APRec *h_aps = nullptr;
+  unsigned long long *h_job_counts = nullptr;
+  // graphs
+  cudaGraphExec_t chunk_graph = nullptr;
+  long long graph_key = -1;
+  // serving
+  std::deque<ServeUnit> units;
+  std::deque<ServeUnit> finished;
+  int64_t bytes_in_use = 0;     // device bytes held by admitted serving units
+  std::string last_error;
+};
+
+static int cuda_fail(ap26_ctx *ctx, cudaError_t e, const char *what) {
+  if (ctx) ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return AP26_E_CUDA;
+}
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+extern "C" int ap26_version(void) { return 10000; }
+
+extern "C" const char *ap26_strerror(int code) {
+  switch (code) {
+    case AP26_OK: return "ok";
+    case AP26_E_ARG: return "bad argument";
+    case AP26_E_CAPACITY: return "output buffer too small";
+    case AP26_E_CUDA: return "CUDA error";
+    case AP26_E_DOMAIN: return "K or SHIFT outside the exact-arithmetic domain";
+    case AP26_E_TIMEOUT: return "device wait timed out";
+    case AP26_E_OVERFLOW: return "internal device buffer overflow";
+    case AP26_E_NOMEM: return "device memory budget exceeded";
+    case AP26_E_INVALID: return "computation error: AP is not even a base-2 PRP AP";
+    case AP26_E_NODEV: return "no usable CUDA device";
+    default: return "unknown error";
+  }
+}
+
+extern "C" const char *ap26_last_error(const ap26_ctx *ctx) {
+  return ctx ? ctx->last_error.c_str() : "";
+}
+
+static int default_opts(ap26_opts *o) {
+  if (!o->dense_primes) o->dense_primes = kVariants[0].G;
+  if (!o->warp_queue) o->warp_queue = kVariants[0].QCAP;
+  if (!o->block_threads) o->block_threads = kVariants[0].WARPS * 32;
+  if (!o->chunk_tiles) o->chunk_tiles = 32768;
+  if (!o->mem_budget) o->mem_budget = (int64_t)8 << 30;
+  return 0;
+}
+
+static int pick_variant(const ap26_opts &o, int sl_hint) {
+  int best = -1;
+  for (int i = 0; i < kNumVariants; i++) {
+    const SieveVariant &v = kVariants[i];
+    if (v.G == o.dense_primes && v.QCAP == o.warp_queue && v.WARPS * 32 == o.block_threads &&
+        (sl_hint <= 0 || v.SL == sl_hint)) {
+      if (best < 0 || v.SL == 44) best = i;
+    }
+  }
+  return best;
+}
+
+static int set_variant(ap26_ctx *ctx, int vi) {
+  const SieveVariant &v = kVariants[vi];
+  CK(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem()));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.kernel, v.WARPS * 32, v.smem()));
+  if (per_sm < 1) per_sm = 1;
+  ctx->variant = vi;
+  ctx->sieve_blocks = ctx->num_sms * per_sm;
+  ctx->opts.dense_primes = v.G;
+  ctx->opts.warp_queue = v.QCAP;
+  ctx->opts.block_threads = v.WARPS * 32;
+  if (ctx->chunk_graph) {
+    cudaGraphExecDestroy(ctx->chunk_graph);
+    ctx->chunk_graph = nullptr;
+  }
+  return AP26_OK;
+}
+
+static int ensure_jobs(ap26_ctx *ctx, int njobs) {
+  if (njobs <= ctx->jobs_cap) return AP26_OK;
+  int cap = std::max(njobs, std::max(64, ctx->jobs_cap * 2));
+  const int64_t need = (int64_t)cap * (sizeof(KJob) + TABLE_WORDS * 4 + 8);
+  if (cap > 64 && need > ctx->opts.mem_budget) return AP26_E_NOMEM;
+  if (ctx->d_jobs) {
+    cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
+    cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts);
+  }
+  CK(cudaMalloc(&ctx->d_jobs, sizeof(KJob) * cap));
+  CK(cudaMalloc(&ctx->d_tables, sizeof(uint32_t) * TABLE_WORDS * (size_t)cap));
+  CK(cudaMalloc(&ctx->d_job_counts, sizeof(unsigned long long) * cap));
+  CK(cudaMallocHost(&ctx->h_jobs, sizeof(KJob) * cap));
+  CK(cudaMallocHost(&ctx->h_job_counts, sizeof(unsigned long long) * cap));
+  ctx->jobs_cap = cap;
+  if (ctx->chunk_graph) {
+    cudaGraphExecDestroy(ctx->chunk_graph);
+    ctx->chunk_graph = nullptr;
+  }
+  return AP26_OK;
+}
+
+extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
+  if (!out) return AP26_E_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    return AP26_E_NODEV;
+  ap26_ctx *ctx = new ap26_ctx();
+  ctx->device = device;
+  if (opts) ctx->opts = *opts;
+  default_opts(&ctx->opts);
+  int rc;
+#define CKC(call)                                     \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) { rc = cuda_fail(ctx, e_, #call); goto fail; } \
+  } while (0)
+  {
+    CKC(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CKC(cudaGetDeviceProperties(&prop, device));
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->chain_blocks = prop.multiProcessorCount * 8;
+    CKC(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CKC(cudaEventCreate(&ctx->ev0));
+    CKC(cudaEventCreate(&ctx->ev1));
+    // constant tables
+    uint16_t trip[NUM_TRIPLES];
+    int nt = ap26h_triples(trip);
+    if (nt != NUM_TRIPLES) { rc = AP26_E_ARG; goto fail; }
+    CKC(cudaMemcpyToSymbol(c_triples, trip, sizeof(trip)));
+    PrimeParam params[NPRIMES];
+    for (int g = 0; g < NPRIMES; g++) params[g] = make_param(g);
+    CKC(cudaMemcpyToSymbol(c_params, params, sizeof(params)));
+    // buffers
+    ctx->cand_cap = 8ll << 20;
+    ctx->ap_cap = 1ll << 20;
+    CKC(cudaMalloc(&ctx->d_st, sizeof(DevState)));
+    CKC(cudaMalloc(&ctx->d_cand, sizeof(Cand) * ctx->cand_cap));
+    CKC(cudaMalloc(&ctx->d_aps, sizeof(APRec) * ctx->ap_cap));
+    CKC(cudaMallocHost(&ctx->h_st, sizeof(DevState)));
+    CKC(cudaMallocHost(&ctx->h_aps, sizeof(APRec) * ctx->ap_cap));
+    if ((rc = ensure_jobs(ctx, 64)) != AP26_OK) goto fail;
+    int vi = pick_variant(ctx->opts, 0);
+    if (vi < 0) { rc = AP26_E_ARG; goto fail; }
+    if ((rc = set_variant(ctx, vi)) != AP26_OK) goto fail;
+  }
+  *out = ctx;
+  return AP26_OK;
+fail:
+  ap26_destroy(ctx);
+  return rc;
+#undef CKC
+}
+
+extern "C" void ap26_destroy(ap26_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
+  cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
+  cudaFree(ctx->d_st); cudaFree(ctx->d_cand); cudaFree(ctx->d_aps);
+  cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts);
+  cudaFreeHost(ctx->h_st); cudaFreeHost(ctx->h_aps);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" int ap26_get_opts(const ap26_ctx *ctx, ap26_opts *out) {
+  if (!ctx || !out) return AP26_E_ARG;
+  *out = ctx->opts;
+  return AP26_OK;
+}
+
+static bool k_in_domain(int K, int shift) {
+  return K >= 1 && K <= AP26_KMAX_SAFE && shift >= 0 && shift <= AP26_SHIFT_MAX;
+}
+
+// Bounded host wait on the stream: polls an event, gives up after timeout_s.
+static int wait_stream(ap26_ctx *ctx, double timeout_s) {
+  cudaEvent_t e = ctx->ev1;
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t q = cudaEventQuery(e);
+    if (q == cudaSuccess) return AP26_OK;
+    if (q != cudaErrorNotReady) return cuda_fail(ctx, q, "cudaEventQuery");
+    double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > timeout_s) {
+      ctx->last_error = "device wait exceeded the timeout";
+      return AP26_E_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 20 : 200));
+  }
+}
+
+// Enqueues the chunked pipeline for ctx->h_jobs[0..njobs) (K, shift, q range
+// and item filled by the caller).  count_only: survivors are counted, no
+// chain walk.  Returns after the D2H of state, counts and reports.
+static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
+                    long long *n_aps_out) {
+  int rc;
+  if ((rc = ensure_jobs(ctx, njobs)) != AP26_OK) return rc;
+  // tile prefix
+  unsigned long long tiles = 0;
+  for (int j = 0; j < njobs; j++) {
+    KJob &J = ctx->h_jobs[j];
+    const int64_t span = J.q_end - J.q_begin;
+    J.ntiles = (int32_t)((span + TILE - 1) / TILE);
+    J.tile_begin = (int64_t)tiles;
+    tiles += (unsigned long long)J.ntiles;
+  }
+  const SieveVariant &V = kVariants[ctx->variant];
+  memset(ctx->h_st, 0, sizeof(DevState));
+  ctx->h_st->chunk_size = (unsigned long long)ctx->opts.chunk_tiles;
+  ctx->h_st->total_tiles = tiles;
+  cudaStream_t s = ctx->stream;
+  CK(cudaEventRecord(ctx->ev0, s));
+  CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob) * njobs, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(ctx->d_job_counts, 0, sizeof(unsigned long long) * njobs, s));
+  setup_jobs_kernel<<<njobs, 256, 0, s>>>(ctx->d_jobs, njobs, ctx->d_tables);
+  CK(cudaGetLastError());
+  int launches = 1;
+  SieveArgs sa{ctx->d_jobs, njobs, ctx->d_tables, ctx->d_st, ctx->d_cand, ctx->cand_cap,
+               ctx->d_job_counts, count_only ? 1 : 0};
+  ChainArgs ca{ctx->d_jobs, ctx->d_st, ctx->d_cand, ctx->cand_cap, ctx->d_aps, ctx->ap_cap};
+  const unsigned long long nchunks =
+      tiles ? (tiles + ctx->opts.chunk_tiles - 1) / ctx->opts.chunk_tiles : 0;
+  const bool use_graph = ctx->opts.use_graphs != 0;
+  const long long key = ((long long)ctx->variant << 40) | ((long long)(count_only ? 1 : 0) << 32) |
+                        (long long)njobs;
+  if (use_graph && (ctx->chunk_graph == nullptr || ctx->graph_key != key)) {
+    if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    chunk_begin_kernel<<<1, 1, 0, cs>>>(ctx->d_st);
+    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), cs>>>(sa);
+    if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, cs>>>(ca);
+    chunk_end_kernel<<<1, 1, 0, cs>>>(ctx->d_st, ctx->cand_cap);
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&ctx->chunk_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaGraphInstantiate");
+    ctx->graph_key = key;
+  }
+  for (unsigned long long c = 0; c < nchunks; c++) {
+    if (use_graph) {
+      CK(cudaGraphLaunch(ctx->chunk_graph, s));
+    } else {
+      chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st);
+      V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+      if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, s>>>(ca);
+      chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap);
+      CK(cudaGetLastError());
+    }
+    launches += count_only ? 3 : 4;
+  }
+  CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ctx->h_job_counts, ctx->d_job_counts, sizeof(unsigned long long) * njobs,
+                     cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(ctx->ev1, s));
+  if ((rc = wait_stream(ctx, 3600.0)) != AP26_OK) return rc;
+  long long n_aps = (long long)std::min<unsigned long long>(ctx->h_st->ap_count, ctx->ap_cap);
+  if (n_aps > 0) {
+    CK(cudaMemcpyAsync(ctx->h_aps, ctx->d_aps, sizeof(APRec) * n_aps, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->candidates = (int64_t)ctx->h_st->cand_total;
+    stats->late_items = (int64_t)ctx->h_st->late_items;
+    stats->prp_tests = (int64_t)ctx->h_st->prp_tests;
+    stats->aps = (int64_t)ctx->h_st->ap_count;
+    stats->device_ms = ms;
+    stats->error_flags = (int32_t)ctx->h_st->err_flags;
+    stats->launches = launches;
+  }
+  if (count_only) {
+    // count-only runs have no candidate buffer use: totals come from job counts
+    unsigned long long tot = 0;
+    for (int j = 0; j < njobs; j++) tot += ctx->h_job_counts[j];
+    if (stats) stats->candidates = (int64_t)tot;
+  }
+  if (n_aps_out) *n_aps_out = n_aps;
+  const unsigned err = ctx->h_st->err_flags;
+  if (err & ERR_DOMAIN) {
+    ctx->last_error = "chain term reached 2^62";
+    return AP26_E_DOMAIN;
+  }
+  if (err & (ERR_CAND_OVERFLOW | ERR_AP_OVERFLOW)) {
+    ctx->last_error = "device buffer overflow";
+    return AP26_E_OVERFLOW;
+  }
+  return AP26_OK;
+}
+
+static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1) {
+  memset(&J, 0, sizeof(J));
+  J.K = K;
+  J.shift = shift;
+  J.item = item;
+  J.q_begin = q0;
+  J.q_end = q1;
+}
+
+// Runs jobs, retrying with smaller chunks on a candidate-buffer overflow.
+static int run_jobs_retry(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
+                          long long *n_aps) {
+  const int saved = ctx->opts.chunk_tiles;
+  std::vector<KJob> keep(ctx->h_jobs, ctx->h_jobs + njobs);
+  int rc = run_jobs(ctx, njobs, count_only, stats, n_aps);
+  int tries = 0;
+  while (rc == AP26_E_OVERFLOW && (ctx->h_st->err_flags & ERR_CAND_OVERFLOW) &&
+         ctx->opts.chunk_tiles > 64 && tries < 6) {
+    ctx->opts.chunk_tiles /= 4;
+    if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
+    memcpy(ctx->h_jobs, keep.data(), sizeof(KJob) * njobs);
+    rc = run_jobs(ctx, njobs, count_only, stats, n_aps);
+    if (stats) stats->error_flags |= 1;
+    tries++;
+  }
+  if (ctx->opts.chunk_tiles != saved) {
+    ctx->opts.chunk_tiles = saved;
+    if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
+  }
+  return rc;
+}
+
+static void aprec_to_ap(const ap26_ctx *ctx, const APRec &r, ap26_ap &a) {
+  a.k = r.k;
+  a.K = ctx->h_jobs[r.job].K;
+  a.first = r.first;
+  a.n = r.n;
+}
+
+extern "C" int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int cap,
+                             int *n_out, ap26_stats *stats) {
+  if (!ctx || !n_out || (cap > 0 && !out)) return AP26_E_ARG;
+  if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
+  if (!ap26_will_search(K)) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K);
+  long long n = 0;
+  int rc = run_jobs_retry(ctx, 1, false, stats, &n);
+  if (rc != AP26_OK) return rc;
+  *n_out = (int)n;
+  if (n > cap) return AP26_E_CAPACITY;
+  for (long long i = 0; i < n; i++) aprec_to_ap(ctx, ctx->h_aps[i], out[i]);
+  ap26_sort_aps(out, (int)n, shift);
+  return AP26_OK;
+}
+
+// ---- batched persistent form ------------------------------------------------------
+extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
+                                 ap26_ap *aps, int64_t ap_cap, int64_t *n_aps,
+                                 ap26_item_result *res, ap26_stats *stats) {
+  if (!ctx || !items || n_items < 0 || !n_aps || !res) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<std::pair<int, int>> jobs;   // (item, K)
+  for (int i = 0; i < n_items; i++) {
+    const ap26_item &it = items[i];
+    if (it.kmax < it.kmin || !k_in_domain(it.kmin, it.shift) || !k_in_domain(it.kmax, it.shift))
+      return AP26_E_DOMAIN;
+    for (int K = it.kmin; K <= it.kmax; K++)
+      if (ap26_will_search(K)) jobs.push_back({i, K});
+  }
+  int rc;
+  if ((rc = ensure_jobs(ctx, (int)jobs.size())) != AP26_OK) return rc;
+  for (size_t j = 0; j < jobs.size(); j++)
+    fill_job(ctx->h_jobs[j], jobs[j].second, items[jobs[j].first].shift, jobs[j].first, 0,
+             N53_PER_K);
+  long long n = 0;
+  if (!jobs.empty()) {
+    rc = run_jobs_retry(ctx, (int)jobs.size(), false, stats, &n);
+    if (rc != AP26_OK) return rc;
+  } else if (stats) {
+    memset(stats, 0, sizeof(*stats));
+  }
+  // group reports: item, K ascending, AVX2 order inside K
+  std::vector<std::vector<ap26_ap>> per_item(n_items);
+  for (long long i = 0; i < n; i++) {
+    const APRec &r = ctx->h_aps[i];
+    ap26_ap a;
+    aprec_to_ap(ctx, r, a);
+    per_item[ctx->h_jobs[r.job].item].push_back(a);
+  }
+  int64_t total = 0;
+  for (int i = 0; i < n_items; i++) {
+    auto &v = per_item[i];
+    std::stable_sort(v.begin(), v.end(), [](const ap26_ap &x, const ap26_ap &y) { return x.K < y.K; });
+    size_t b = 0;
+    while (b < v.size()) {
+      size_t e = b;
+      while (e < v.size() && v[e].K == v[b].K) e++;
+      ap26_sort_aps(v.data() + b, (int)(e - b), items[i].shift);
+      b = e;
+    }
+    res[i].id = items[i].id;
+    res[i].status = AP26_OK;
+    res[i].n_aps = (int32_t)v.size();
+    res[i].first_ap = total;
+    res[i].candidates = 0;
+    res[i].ks_searched = 0;
+    res[i].latency_ms = 0;
+    total += (int64_t)v.size();
+  }
+  for (size_t j = 0; j < jobs.size(); j++) {
+    res[jobs[j].first].candidates += (int64_t)ctx->h_job_counts[j];
+    res[jobs[j].first].ks_searched++;
+  }
+  *n_aps = total;
+  if (total > ap_cap) return AP26_E_CAPACITY;
+  for (int i = 0; i < n_items; i++)
+    if (!per_item[i].empty())
+      memcpy(aps + res[i].first_ap, per_item[i].data(), sizeof(ap26_ap) * per_item[i].size());
+  return AP26_OK;
+}
+
+// ---- serving: continuous batching ----------------------------------------------------
+// A unit costs its K-job tables and descriptors while admitted.
+static int64_t unit_bytes(size_t nk) { return (int64_t)nk * (TABLE_WORDS * 4 + sizeof(KJob) + 8); }
+
+extern "C" int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item) {
+  if (!ctx || !item || item->kmax < item->kmin) return AP26_E_ARG;
+  if (!k_in_domain(item->kmin, item->shift) || !k_in_domain(item->kmax, item->shift))
+    return AP26_E_DOMAIN;
+  ServeUnit u;
+  u.item = *item;
+  for (int K = item->kmin; K <= item->kmax; K++)
+    if (ap26_will_search(K)) u.ks.push_back(K);
+  const int64_t need = unit_bytes(u.ks.size());
+  if (ctx->bytes_in_use + need > ctx->opts.mem_budget) return AP26_E_NOMEM;
+  ctx->bytes_in_use += need;
+  u.t_submit = std::chrono::steady_clock::now();
+  ctx->units.push_back(std::move(u));
+  return AP26_OK;
+}
+
+// One slice: up to `slice_k` K-jobs drawn round-robin from the admitted units
+// run as one batched launch chain; finished units move to the poll queue.
+extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
+  if (!ctx) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const int slice_k = std::max(1, ctx->num_sms / 8);
+  std::vector<std::pair<ServeUnit *, int>> picked;
+  bool progress = true;
+  while ((int)picked.size() < slice_k && progress) {
+    progress = false;
+    for (auto &u : ctx->units) {
+      if ((int)picked.size() >= slice_k) break;
+      if (u.next_k < u.ks.size()) {
+        picked.push_back({&u, u.ks[u.next_k++]});
+        progress = true;
+      }
+    }
+  }
+  if (!picked.empty()) {
+    int rc;
+    if ((rc = ensure_jobs(ctx, (int)picked.size())) != AP26_OK) return rc;
+    for (size_t j = 0; j < picked.size(); j++)
+      fill_job(ctx->h_jobs[j], picked[j].second, picked[j].first->item.shift, (int)j, 0,
+               N53_PER_K);
+    long long n = 0;
+    ap26_stats st;
+    rc = run_jobs_retry(ctx, (int)picked.size(), false, &st, &n);
+    if (rc != AP26_OK) {
+      for (auto &pk : picked) pk.first->status = rc;
+    } else {
+      std::vector<std::vector<ap26_ap>> per_job(picked.size());
+      for (long long i = 0; i < n; i++) {
+        ap26_ap a;
+        aprec_to_ap(ctx, ctx->h_aps[i], a);
+        per_job[ctx->h_aps[i].job].push_back(a);
+      }
+      for (size_t j = 0; j < picked.size(); j++) {
+        ServeUnit *u = picked[j].first;
+        ap26_sort_aps(per_job[j].data(), (int)per_job[j].size(), u->item.shift);
+        u->aps.insert(u->aps.end(), per_job[j].begin(), per_job[j].end());
+        u->candidates += (int64_t)ctx->h_job_counts[j];
+        u->done_k++;
+      }
+    }
+  }
+  for (auto it = ctx->units.begin(); it != ctx->units.end();) {
+    if (it->done_k == (int)it->ks.size() || it->status != AP26_OK) {
+      it->latency_ms = std::chrono::duration<double, std::milli>(
+                           std::chrono::steady_clock::now() - it->t_submit).count();
+      ctx->bytes_in_use -= unit_bytes(it->ks.size());
+      ctx->finished.push_back(std::move(*it));
+      it = ctx->units.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  if (active_units) *active_units = (int)ctx->units.size();
+  return AP26_OK;
+}
+
+extern "C" int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *aps,
+                               int64_t ap_cap, int64_t *n_aps) {
+  if (!ctx || !res || !n_aps) return AP26_E_ARG;
+  if (ctx->finished.empty()) return 0;
+  ServeUnit &u = ctx->finished.front();
+  *n_aps = (int64_t)u.aps.size();
+  if ((int64_t)u.aps.size() > ap_cap) return AP26_E_CAPACITY;
+  if (!u.aps.empty()) memcpy(aps, u.aps.data(), sizeof(ap26_ap) * u.aps.size());
+  res->id = u.item.id;
+  res->status = u.status;
+  res->n_aps = (int32_t)u.aps.size();
+  res->first_ap = 0;
+  res->candidates = u.candidates;
+  res->ks_searched = (int32_t)u.ks.size();
+  res->latency_ms = u.latency_ms;
+  ctx->finished.pop_front();
+  return 1;
+}
+
+// ---- kernel-level entry points ---------------------------------------------------------
+extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin, int64_t q_end,
+                                int64_t *cand, int64_t cap, int64_t *n_cand, ap26_stats *stats) {
+  if (!ctx || !n_cand || q_begin < 0 || q_end > N53_PER_K || q_end < q_begin) return AP26_E_ARG;
+  if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
+  CK(cudaSetDevice(ctx->device));
+  fill_job(ctx->h_jobs[0], K, shift, 0, q_begin, q_end);
+  // sieve without the chain walk: one chunk covering everything, candidates kept
+  const int saved = ctx->opts.chunk_tiles;
+  const int64_t tiles = (q_end - q_begin + TILE - 1) / TILE;
+  ctx->opts.chunk_tiles = (int)std::max<int64_t>(1, tiles);
+  if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
+  const int saved_graph = ctx->opts.use_graphs;
+  ctx->opts.use_graphs = 0;
+  // run setup + sieve only (no chain) by hand
+  int rc = AP26_OK;
+  {
+    KJob &J = ctx->h_jobs[0];
+    J.ntiles = (int32_t)tiles;
+    J.tile_begin = 0;
+    memset(ctx->h_st, 0, sizeof(DevState));
+    ctx->h_st->chunk_size = (unsigned long long)std::max<int64_t>(1, tiles);
+    ctx->h_st->total_tiles = (unsigned long long)tiles;
+    cudaStream_t s = ctx->stream;
+    const SieveVariant &V = kVariants[ctx->variant];
+    CK(cudaEventRecord(ctx->ev0, s));
+    CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(ctx->d_job_counts, 0, sizeof(unsigned long long), s));
+    setup_jobs_kernel<<<1, 256, 0, s>>>(ctx->d_jobs, 1, ctx->d_tables);
+    chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st);
+    SieveArgs sa{ctx->d_jobs, 1, ctx->d_tables, ctx->d_st, ctx->d_cand, ctx->cand_cap,
+                 ctx->d_job_counts, 0};
+    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(ctx->ev1, s));
+    rc = wait_stream(ctx, 3600.0);
+    if (rc == AP26_OK) {
+      const long long nc = (long long)ctx->h_st->cand_count;
+      *n_cand = nc;
+      if (nc > ctx->cand_cap) rc = AP26_E_OVERFLOW;
+      else if (nc > cap) rc = AP26_E_CAPACITY;
+      else if (nc > 0) {
+        std::vector<Cand> tmp(nc);
+        CK(cudaMemcpy(tmp.data(), ctx->d_cand, sizeof(Cand) * nc, cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < nc; i++) cand[i] = tmp[i].n;
+      }
+      if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        memset(stats, 0, sizeof(*stats));
+        stats->candidates = nc;
+        stats->late_items = (int64_t)ctx->h_st->late_items;
+        stats->device_ms = ms;
+        stats->error_flags = (int32_t)ctx->h_st->err_flags;
+        stats->launches = 3;
+      }
+    }
+  }
+  ctx->opts.chunk_tiles = saved;
+  ctx->opts.use_graphs = saved_graph;
+  return rc;
+}
+
+extern "C" int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int shift,
+                                int64_t *counts, ap26_stats *stats) {
+  if (!ctx || !Ks || nK <= 0 || !counts) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure_jobs(ctx, nK)) != AP26_OK) return rc;
+  for (int i = 0; i < nK; i++) {
+    if (!k_in_domain(Ks[i], shift)) return AP26_E_DOMAIN;
+    fill_job(ctx->h_jobs[i], Ks[i], shift, i, 0, N53_PER_K);
+  }
+  rc = run_jobs(ctx, nK, true, stats, nullptr);
+  if (rc != AP26_OK) return rc;
+  for (int i = 0; i < nK; i++) counts[i] = (int64_t)ctx->h_job_counts[i];
+  return AP26_OK;
+}
+
+extern "C" int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count, uint8_t *verdict,
+                               ap26_stats *stats) {
+  if (!ctx || !N || !verdict || count < 0) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (count == 0) return AP26_OK;
+  uint64_t *dN = nullptr;
+  uint8_t *dV = nullptr;
+  unsigned long long *dsq = nullptr, hsq = 0;
+  CK(cudaMalloc(&dN, sizeof(uint64_t) * count));
+  CK(cudaMalloc(&dV, count));
+  CK(cudaMalloc(&dsq, sizeof(unsigned long long)));
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(dsq, 0, sizeof(unsigned long long), s));
+  CK(cudaMemcpyAsync(dN, N, sizeof(uint64_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev0, s));
+  sprp_batch_kernel<<<ctx->num_sms * 16, 256, 0, s>>>(dN, count, dV, dsq);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev1, s));
+  CK(cudaMemcpyAsync(verdict, dV, count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&hsq, dsq, sizeof(hsq), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->prp_tests = count;
+    stats->device_ms = ms;
+    stats->late_items = (int64_t)hsq;   // modular squarings performed
+    stats->launches = 1;
+  }
+  cudaFree(dN); cudaFree(dV); cudaFree(dsq);
+  return AP26_OK;
+}
+
+extern "C" int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
+                                int32_t *k_out, int64_t *first_out, ap26_stats *stats) {
+  if (!ctx || (count > 0 && (!n || !k_out || !first_out)) || count < 0) return AP26_E_ARG;
+  if (!k_in_domain(K, 0)) return AP26_E_DOMAIN;
+  CK(cudaSetDevice(ctx->device));
+  if (count == 0) return AP26_OK;
+  fill_job(ctx->h_jobs[0], K, 0, 0, 0, 0);
+  int64_t *dn = nullptr, *df = nullptr;
+  int32_t *dk = nullptr;
+  CK(cudaMalloc(&dn, sizeof(int64_t) * count));
+  CK(cudaMalloc(&df, sizeof(int64_t) * count));
+  CK(cudaMalloc(&dk, sizeof(int32_t) * count));
+  cudaStream_t s = ctx->stream;
+  memset(ctx->h_st, 0, sizeof(DevState));
+  CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+  setup_jobs_kernel<<<1, 256, 0, s>>>(ctx->d_jobs, 1, ctx->d_tables);
+  CK(cudaMemcpyAsync(dn, n, sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev0, s));
+  chain_explicit_kernel<<<ctx->num_sms * 8, 128, 0, s>>>(ctx->d_jobs, dn, count, dk, df, ctx->d_st);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev1, s));
+  CK(cudaMemcpyAsync(k_out, dk, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(first_out, df, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->device_ms = ms;
+    stats->error_flags = (int32_t)ctx->h_st->err_flags;
+    stats->launches = 2;
+  }
+  cudaFree(dn); cudaFree(df); cudaFree(dk);
+  return (ctx->h_st->err_flags & ERR_DOMAIN) ? AP26_E_DOMAIN : AP26_OK;
+}
+
+extern "C" int ap26_probe_peaks(ap26_ctx *ctx, double *smem_gbs, double *int_tops) {
+  if (!ctx) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  unsigned *sink = nullptr;
+  CK(cudaMalloc(&sink, sizeof(unsigned)));
+  cudaStream_t s = ctx->stream;
+  const int blocks = ctx->num_sms * 4, threads = 256;
+  const int siters = 4096, iiters = 4096;
+  float ms = 0;
+  for (int rep = 0; rep < 2; rep++) {
+    CK(cudaEventRecord(ctx->ev0, s));
+    smem_probe_kernel<<<blocks, threads, 0, s>>>(siters, sink);
+    CK(cudaEventRecord(ctx->ev1, s));
+    CK(cudaEventSynchronize(ctx->ev1));
+  }
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (smem_gbs) *smem_gbs = (double)blocks * threads * siters * 8 * 16 / (ms * 1e-3) / 1e9;
+  for (int rep = 0; rep < 2; rep++) {
+    CK(cudaEventRecord(ctx->ev0, s));
+    int_probe_kernel<<<blocks, threads, 0, s>>>(iiters, sink);
+    CK(cudaEventRecord(ctx->ev1, s));
+    CK(cudaEventSynchronize(ctx->ev1));
+  }
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  // one IMAD (a*m + c) per element per step: 8 * 16 per iteration
+  if (int_tops) *int_tops = (double)blocks * threads * iiters * 8 * 16 / (ms * 1e-3) / 1e12;
+  cudaFree(sink);
+  return AP26_OK;
+}
+
+// ---- autotuner -------------------------------------------------------------------------------
+// Times every compiled sieve variant (and two chunk sizes) on the same slice
+// of K's lattice (count-only, so only the sieve is measured) and keeps the
+// fastest.  The slice is the first 1/64 of the K's starts.
+extern "C" int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen) {
+  if (!ctx) return AP26_E_ARG;
+  if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
+  CK(cudaSetDevice(ctx->device));
+  const int64_t q1 = N53_PER_K / 64;
+  double best_ms = 1e30;
+  int best_v = ctx->variant, best_chunk = ctx->opts.chunk_tiles;
+  const int chunks[2] = {8192, 32768};
+  for (int vi = 0; vi < kNumVariants; vi++) {
+    int rc = set_variant(ctx, vi);
+    if (rc != AP26_OK) return rc;
+    for (int ci = 0; ci < 2; ci++) {
+      ctx->opts.chunk_tiles = chunks[ci];
+      double t = 0;
+      for (int rep = 0; rep < 2; rep++) {
+        fill_job(ctx->h_jobs[0], K, shift, 0, 0, q1);
+        ap26_stats st;
+        rc = run_jobs(ctx, 1, true, &st, nullptr);
+        if (rc != AP26_OK) return rc;
+        if (rep == 1) t = st.device_ms;   // first run warms up
+      }
+      if (t < best_ms) { best_ms = t; best_v = vi; best_chunk = chunks[ci]; }
+    }
+  }
+  int rc = set_variant(ctx, best_v);
+  ctx->opts.chunk_tiles = best_chunk;
+  if (chosen) *chosen = ctx->opts;
+  return rc;
+}

@@ -1,0 +1,525 @@
+// ap26_kernels.cuh -- sm_100a kernels of the AP26 per-K search.
+//
+// Pipeline for a set of K-jobs (one (K, SHIFT) pair each), run chunk by chunk
+// on one stream (ap26_capi.cu):
+//
+//   setup_jobs_kernel   per-K residue setup (the reference's split
+//                       multiplications, src/opencl/AP26.h:112-120) and the
+//                       per-K sieve bitstrings (replaces clearok/setok/
+//                       setupokok/offset, src/opencl/kernels/*.cl)
+//   chunk_begin_kernel  resets per-chunk counters
+//   sieve_kernel        persistent, work-stealing over 256-start tiles;
+//                       replaces setupn.cl + sieve.cl (the 1.1 GB n59 array
+//                       of the reference is never materialised: starts are
+//                       generated from a flat index)
+//   chain_kernel        base-2 SPRP chain walk (replaces checkn.cl)
+//   chunk_end_kernel    advances the chunk window
+//
+// ---------------------------------------------------------------------------
+// Sieve formulation.  The reference ANDs, for every lattice value n59 and
+// every shift word w (absolute shift SHIFT+64w), the 83 table words
+// OKOK_{p,w}[n59 mod p] (sieve.cl:238-320), where bit b of OKOK_{p,w}[r] is
+// OK_p[(r + (SHIFT+64w+b)*MOD) mod p] (setupokok.cl, cpusse2.cpp:38-43).
+// Multiplying the index by MOD^-1 mod p turns the 640 bits of all 10 words
+// into ONE window of a p-periodic bitstring:
+//     B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
+//     bit i of the 640-bit mask = B_p[s + i],  s = n59 * MOD^-1 mod p.
+// So each prime needs a (p + 672)-bit string (10 KB for all 83 primes, kept
+// in shared memory) and, per n59, one window offset.  Reading the window is
+// conflict-free: all lanes read the same prime's string at word offsets
+// that differ by at most (p-1)/32 < 17, i.e. inside one 32-bank row.
+//
+//   dense phase  the first G primes for all 10 words of every n59 (21 word
+//                loads + 20 funnel shifts per prime)
+//   tail         live (n59, word) pairs are compacted into a per-warp shared
+//                queue (ballot/popc) and advanced R primes at a time, all
+//                lanes on the same prime, until stage SL
+//   late         the few pairs alive at SL finish lane-by-lane; surviving
+//                bits pass the 7..23 filter (sieve.cl:333-346) and become
+//                candidates n = n59 + (SHIFT + 64w + b) * MOD.
+#pragma once
+#include <stdint.h>
+#include <utility>
+#include "ap26_const.cuh"
+
+namespace ap26 {
+
+// ---- device data ------------------------------------------------------------
+struct KJob {
+  int64_t STEP, n0, S31, S37, S41, S43, S47, S53, S59;
+  int64_t q_begin, q_end;     // n53 start range [q_begin, q_end)
+  int64_t tile_begin;         // global index of this job's first tile
+  int32_t K, shift, item, ntiles;
+};
+
+struct Cand {
+  int64_t n;
+  int32_t job;
+  int32_t pad;
+};
+
+struct APRec {
+  int32_t k;
+  int32_t job;
+  int64_t first;
+  int64_t n;
+};
+
+struct DevState {
+  unsigned long long tile_next, tile_end;      // current chunk window
+  unsigned long long chunk_begin, chunk_size, total_tiles;
+  unsigned long long cand_count;               // per chunk
+  unsigned long long ap_count, prp_tests, cand_total, late_items;  // per run
+  unsigned int err_flags;
+  unsigned int pad;
+};
+
+enum : unsigned int {
+  ERR_CAND_OVERFLOW = 1u,
+  ERR_DOMAIN = 4u,
+  ERR_AP_OVERFLOW = 8u,
+};
+
+struct SieveArgs {
+  const KJob *jobs;
+  int njobs;
+  const uint32_t *tables;       // [njobs][TABLE_WORDS]
+  DevState *st;
+  Cand *cand;
+  long long cand_cap;
+  unsigned long long *job_counts;  // per-job survivor counts
+  int count_only;               // 1: count survivors, emit no candidates
+};
+
+struct ChainArgs {
+  const KJob *jobs;
+  DevState *st;
+  const Cand *cand;
+  long long cand_cap;
+  APRec *aps;
+  long long ap_cap;
+};
+
+constexpr int TILE = 256;          // n53 starts per tile
+constexpr uint32_t FULL = 0xffffffffu;
+
+// (i31, i37, i41) triples in the reference's loop order (AP26.h:127-131),
+// packed 5 bits each, and the per-prime parameters; filled by the host.
+// (This header is compiled into exactly one translation unit.)
+__constant__ uint16_t c_triples[NUM_TRIPLES];
+__constant__ PrimeParam c_params[NPRIMES];
+
+// ---- 64-bit helpers -----------------------------------------------------------
+// x mod MOD for 0 <= x < 2^62 via a double quotient estimate corrected once
+// (the estimate is within one of floor(x/MOD)).
+__device__ __forceinline__ int64_t mod_MOD(uint64_t x) {
+  const double inv = 1.0 / (double)MOD;
+  int64_t q = (int64_t)((double)x * inv);
+  int64_t r = (int64_t)x - q * MOD;
+  if (r < 0) r += MOD;
+  else if (r >= MOD) r -= MOD;
+  return r;
+}
+
+// ---- sieve pieces -----------------------------------------------------------
+template <int g>
+__device__ __forceinline__ uint32_t window_start(uint32_t a, uint32_t b, uint32_t c) {
+  constexpr PrimeParam P = make_param(g);
+  uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
+  return x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
+}
+
+// All 640 bits (20 words) of prime g ANDed into acc.
+template <int g>
+__device__ __forceinline__ void dense_prime(const uint32_t *__restrict__ tab, uint32_t a,
+                                            uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
+  constexpr PrimeParam P = make_param(g);
+  uint32_t s = window_start<g>(a, b, c);
+  const uint32_t *t = tab + P.off + (s >> 5);
+  uint32_t sh = s & 31;
+  uint32_t v[21];
+#pragma unroll
+  for (int i = 0; i < 21; i++) v[i] = t[i];
+#pragma unroll
+  for (int i = 0; i < 20; i++) acc[i] &= __funnelshift_r(v[i], v[i + 1], sh);
+}
+
+template <int... I>
+__device__ __forceinline__ void dense_all(const uint32_t *tab, uint32_t a, uint32_t b,
+                                          uint32_t c, uint32_t (&acc)[20],
+                                          std::integer_sequence<int, I...>) {
+  (dense_prime<I>(tab, a, b, c, acc), ...);
+}
+
+// One word (64 bits starting at bit 64*w of the window) of prime g.
+template <int g>
+__device__ __forceinline__ void word_prime(const uint32_t *__restrict__ tab, uint32_t a,
+                                           uint32_t b, uint32_t c, uint32_t w64,
+                                           uint32_t &lo, uint32_t &hi) {
+  if constexpr (g < NPRIMES) {
+    constexpr PrimeParam P = make_param(g);
+    uint32_t pos = window_start<g>(a, b, c) + w64;
+    const uint32_t *t = tab + P.off + (pos >> 5);
+    uint32_t sh = pos & 31;
+    uint32_t v0 = t[0], v1 = t[1], v2 = t[2];
+    lo &= __funnelshift_r(v0, v1, sh);
+    hi &= __funnelshift_r(v1, v2, sh);
+  }
+}
+
+// Same with runtime prime index (late stage; all active lanes share g).
+__device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab, int g,
+                                              uint32_t a, uint32_t b, uint32_t c,
+                                              uint32_t w64, uint32_t &lo, uint32_t &hi) {
+  const PrimeParam P = c_params[g];
+  uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
+  uint32_t s = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
+  uint32_t pos = s + w64;
+  const uint32_t *t = tab + P.off + (pos >> 5);
+  uint32_t sh = pos & 31;
+  uint32_t v0 = t[0], v1 = t[1], v2 = t[2];
+  lo &= __funnelshift_r(v0, v1, sh);
+  hi &= __funnelshift_r(v1, v2, sh);
+}
+
+// Queue item: x = n59 bits 0..31, y = n59 bits 32..47 | w << 16, z/w = mask.
+__device__ __forceinline__ void split_n59(uint32_t x, uint32_t y, uint32_t &a, uint32_t &b,
+                                          uint32_t &c) {
+  a = x & 0xffffu;
+  b = x >> 16;
+  c = y & 0xffffu;
+}
+
+// Emits the candidates of one fully sieved word: each set bit b gives
+// n = n59 + (shift + 64w + b) * MOD, kept when n has no factor 7..23.
+__device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w, uint64_t mask,
+                                         int shift, int job) {
+  int kept = 0;
+  while (mask) {
+    int b = __ffsll((long long)mask) - 1;
+    mask &= mask - 1;
+    int64_t n = (int64_t)n59 + (int64_t)(shift + 64 * w + b) * MOD;
+    if (n % 7 && n % 11 && n % 13 && n % 17 && n % 19 && n % 23) {
+      kept++;
+      if (!A.count_only) {
+        unsigned long long i = atomicAdd(&A.st->cand_count, 1ull);
+        if ((long long)i < A.cand_cap) {
+          A.cand[i].n = n;
+          A.cand[i].job = job;
+        } else {
+          atomicOr(&A.st->err_flags, ERR_CAND_OVERFLOW);
+        }
+      }
+    }
+  }
+  return kept;
+}
+
+// Tail stage group: advance every queued item through primes g0..g0+R-1 and
+// compact the survivors in place (write index <= read index).
+template <int g0, int R>
+__device__ __forceinline__ void tail_group(const uint32_t *tab, uint4 *q, int &cnt, int lane) {
+  int out = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    int i = base + lane;
+    bool valid = i < cnt;
+    uint4 it = valid ? q[i] : make_uint4(0, 0, 0, 0);
+    __syncwarp();
+    uint32_t a, b, c;
+    split_n59(it.x, it.y, a, b, c);
+    uint32_t w64 = ((it.y >> 16) & 15u) * 64u;
+    uint32_t lo = it.z, hi = it.w;
+    if constexpr (R > 0) word_prime<g0 + 0>(tab, a, b, c, w64, lo, hi);
+    if constexpr (R > 1) word_prime<g0 + 1>(tab, a, b, c, w64, lo, hi);
+    if constexpr (R > 2) word_prime<g0 + 2>(tab, a, b, c, w64, lo, hi);
+    if constexpr (R > 3) word_prime<g0 + 3>(tab, a, b, c, w64, lo, hi);
+    if constexpr (R > 4) word_prime<g0 + 4>(tab, a, b, c, w64, lo, hi);
+    if constexpr (R > 5) word_prime<g0 + 5>(tab, a, b, c, w64, lo, hi);
+    bool alive = valid && ((lo | hi) != 0u);
+    unsigned bal = __ballot_sync(FULL, alive);
+    if (alive) q[out + __popc(bal & ((1u << lane) - 1u))] = make_uint4(it.x, it.y, lo, hi);
+    out += __popc(bal);
+    __syncwarp();
+  }
+  cnt = out;
+}
+
+template <int g0, int R, int SL>
+__device__ __forceinline__ void tail_stages(const uint32_t *tab, uint4 *q, int &cnt, int lane) {
+  if constexpr (g0 < SL) {
+    if (cnt == 0) return;
+    constexpr int r = (g0 + R <= SL) ? R : (SL - g0);
+    tail_group<g0, r>(tab, q, cnt, lane);
+    tail_stages<g0 + r, R, SL>(tab, q, cnt, lane);
+  }
+}
+
+// Runs the queue to completion: stage-synchronous groups up to SL, then the
+// remaining items lane-by-lane through the last primes, then emission.
+template <int G, int R, int SL>
+__device__ __forceinline__ int drain_queue(const SieveArgs &A, const uint32_t *tab, uint4 *q,
+                                           int &cnt, int lane, int shift, int job,
+                                           unsigned long long &late) {
+  tail_stages<G, R, SL>(tab, q, cnt, lane);
+  late += (unsigned long long)cnt;
+  int kept = 0;
+  for (int i = lane; i < cnt; i += 32) {
+    uint4 it = q[i];
+    uint32_t a, b, c;
+    split_n59(it.x, it.y, a, b, c);
+    uint32_t wv = (it.y >> 16) & 15u;
+    uint32_t lo = it.z, hi = it.w;
+    for (int g = SL; g < NPRIMES && (lo | hi); g++)
+      word_prime_rt(tab, g, a, b, c, wv * 64u, lo, hi);
+    if (lo | hi) {
+      uint64_t n59 = (uint64_t)it.x | ((uint64_t)(it.y & 0xffffu) << 32);
+      kept += emit_word(A, n59, (int)wv, ((uint64_t)hi << 32) | lo, shift, job);
+    }
+  }
+  __syncwarp();
+  cnt = 0;
+  return kept;
+}
+
+// n53 start of lattice index q (0 <= q < N53_PER_K) of job J:
+// n43 = (n0 + i3*S3 + i5*S5 + i31*S31 + i37*S37 + i41*S41) mod MOD
+// (AP26.h:134) and n53 = n43 + j43*S43 + j47*S47 + j53*S53 mod MOD, the
+// value the reference's nested increments reach (setupn.cl:31-53).
+__device__ __forceinline__ int64_t n53_at(const KJob &J, int64_t q) {
+  int n43i = (int)(q / N53_PER_N43);
+  int rem = (int)(q - (int64_t)n43i * N53_PER_N43);
+  int j43 = rem / 667;
+  rem -= j43 * 667;
+  int j47 = rem / 29;
+  int j53 = rem - j47 * 29;
+  uint32_t tr = c_triples[n43i >> 3];
+  int i31 = tr & 31, i37 = (tr >> 5) & 31, i41 = (tr >> 10) & 31;
+  int i3 = (n43i >> 2) & 1, i5 = n43i & 3;
+  uint64_t x = (uint64_t)J.n0 + (uint64_t)i3 * (uint64_t)S3 + (uint64_t)i5 * (uint64_t)S5 +
+               (uint64_t)i31 * (uint64_t)J.S31 + (uint64_t)i37 * (uint64_t)J.S37 +
+               (uint64_t)i41 * (uint64_t)J.S41;
+  uint64_t n43 = (uint64_t)mod_MOD(x);
+  uint64_t y = n43 + (uint64_t)j43 * (uint64_t)J.S43 + (uint64_t)j47 * (uint64_t)J.S47 +
+               (uint64_t)j53 * (uint64_t)J.S53;
+  return mod_MOD(y);
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int find_job(const KJob *jobs, int njobs, unsigned long long tile) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if ((unsigned long long)jobs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ---- the sieve kernel -----------------------------------------------------------
+// Persistent: each CTA grabs 256-start tiles from DevState::tile_next until
+// the chunk window ends.  WARPS warps, one start per lane, 35 n59 per start.
+template <int G, int R, int SL, int QCAP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+sieve_kernel(SieveArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
+  uint32_t *tab = reinterpret_cast<uint32_t *>(smem_raw + sizeof(uint4) * QCAP * WARPS);
+  __shared__ unsigned long long s_tile;
+  __shared__ int s_job;
+  __shared__ unsigned long long s_kept[WARPS];
+  __shared__ unsigned long long s_late[WARPS];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint4 *q = queues + warp * QCAP;
+  constexpr int THRESH = QCAP - 32 * WORDS;
+  static_assert(THRESH >= 0, "queue too small for one dense batch");
+
+  int cur_job = -1;
+  unsigned long long kept_acc = 0, late_acc = 0;
+  if (lane == 0) { s_kept[warp] = 0; s_late[warp] = 0; }
+
+  for (;;) {
+    if (threadIdx.x == 0) {
+      unsigned long long t = atomicAdd(&A.st->tile_next, 1ull);
+      s_tile = t;
+      s_job = (t < A.st->tile_end) ? find_job(A.jobs, A.njobs, t) : -1;
+    }
+    __syncthreads();
+    const unsigned long long tile = s_tile;
+    const int job = s_job;
+    if (job < 0) break;
+    if (job != cur_job) {
+      // flush per-job survivor count of the previous job
+      if (cur_job >= 0) {
+        const unsigned long long v = warp_sum(kept_acc);
+        if (lane == 0) s_kept[warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          unsigned long long s = 0;
+          for (int i = 0; i < WARPS; i++) s += s_kept[i];
+          if (s) atomicAdd(&A.job_counts[cur_job], s);
+        }
+        kept_acc = 0;
+      }
+      const uint32_t *src = A.tables + (size_t)job * TABLE_WORDS;
+      for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) tab[i] = src[i];
+      cur_job = job;
+      __syncthreads();
+    }
+    const KJob &J = A.jobs[job];
+    const int shift = J.shift;
+    const int64_t S59 = J.S59;
+    int64_t qi = J.q_begin + (int64_t)(tile - (unsigned long long)J.tile_begin) * TILE +
+                 warp * 32 + lane;
+    const bool valid = qi < J.q_end;
+    int64_t n59 = valid ? n53_at(J, qi) : 0;
+    int cnt = 0;
+    unsigned long long kept = 0;
+
+    for (int j = 0; j < J59; j++) {
+      uint32_t acc[20];
+#pragma unroll
+      for (int i = 0; i < 20; i++) acc[i] = valid ? FULL : 0u;
+      const uint32_t x = (uint32_t)n59, y = (uint32_t)((uint64_t)n59 >> 32);
+      uint32_t a, b, c;
+      split_n59(x, y, a, b, c);
+      dense_all(tab, a, b, c, acc, std::make_integer_sequence<int, G>{});
+#pragma unroll
+      for (int w = 0; w < WORDS; w++) {
+        const uint32_t lo = acc[2 * w], hi = acc[2 * w + 1];
+        const bool live = (lo | hi) != 0u;
+        const unsigned bal = __ballot_sync(FULL, live);
+        if (live)
+          q[cnt + __popc(bal & ((1u << lane) - 1u))] =
+              make_uint4(x, y | ((uint32_t)w << 16), lo, hi);
+        cnt += __popc(bal);
+      }
+      __syncwarp();
+      if (cnt > THRESH) kept += drain_queue<G, R, SL>(A, tab, q, cnt, lane, shift, job, late_acc);
+      n59 += S59;
+      if (n59 >= MOD) n59 -= MOD;
+    }
+    kept += drain_queue<G, R, SL>(A, tab, q, cnt, lane, shift, job, late_acc);
+    kept_acc += kept;
+    __syncthreads();   // all warps done with this tile's table before a reload
+  }
+  // final flush (kept is per lane; late is warp-uniform)
+  const unsigned long long vk = warp_sum(kept_acc);
+  if (lane == 0) { s_kept[warp] = vk; s_late[warp] = late_acc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0, l = 0;
+    for (int i = 0; i < WARPS; i++) { s += s_kept[i]; l += s_late[i]; }
+    if (cur_job >= 0 && s) atomicAdd(&A.job_counts[cur_job], s);
+    if (l) atomicAdd(&A.st->late_items, l);
+  }
+}
+
+// ---- Montgomery arithmetic mod odd N < 2^63 ---------------------------------------
+// REDC with R = 2^64: for a, b < N, t = a*b, m = t_lo * (-N^-1) mod 2^64,
+// (t + m*N) / 2^64 = t_hi + mulhi(m, N) + (t_lo != 0) < 2N.
+__device__ __forceinline__ uint64_t mont_mul(uint64_t a, uint64_t b, uint64_t N, uint64_t ninv) {
+  uint64_t lo = a * b, hi = __umul64hi(a, b);
+  uint64_t m = lo * ninv;
+  uint64_t r = hi + __umul64hi(m, N) + (lo != 0 ? 1ull : 0ull);
+  return r >= N ? r - N : r;
+}
+
+__device__ __forceinline__ uint64_t neg_inv64(uint64_t N) {
+  uint64_t x = N;               // correct to 3 bits for odd N
+#pragma unroll
+  for (int i = 0; i < 5; i++) x *= 2 - N * x;
+  return 0 - x;
+}
+
+// 2^64 mod N by binary long division from N << clz(N) (>= 2^63).
+__device__ __forceinline__ uint64_t r_mod(uint64_t N) {
+  int s = __clzll((long long)N);
+  uint64_t r = 0 - (N << s);
+  for (int i = s - 1; i >= 0; i--)
+    if (r >= (N << i)) r -= (N << i);
+  return r;
+}
+
+// Base-2 strong probable prime test, same verdict as the reference's
+// strong_prp(2, N) (PrimeQ_x86.h:143-182, checkn.cl:59-122) for odd N in
+// [3, 2^63): left-to-right exponentiation by d = (N-1)/2^t in Montgomery
+// form, the multiplications by the base 2 done as modular doublings.
+// *sq counts the modular squarings.
+__device__ __forceinline__ bool sprp2(uint64_t N, unsigned &sq) {
+  if (N < 3) return false;
+  const uint64_t nm1 = N - 1;
+  const int t = __ffsll((long long)nm1) - 1;
+  const uint64_t d = nm1 >> t;
+  const uint64_t ninv = neg_inv64(N);
+  const uint64_t one = r_mod(N);
+  const uint64_t mone = N - one;
+  uint64_t x = one + one;
+  if (x >= N) x -= N;                   // 2 in Montgomery form
+  const int top = 63 - __clzll((long long)d);
+  for (int i = top - 1; i >= 0; i--) {
+    x = mont_mul(x, x, N, ninv);
+    sq++;
+    if ((d >> i) & 1) {
+      x += x;
+      if (x >= N) x -= N;
+    }
+  }
+  if (x == one || x == mone) return true;
+  for (int s = 1; s < t; s++) {
+    x = mont_mul(x, x, N, ninv);
+    sq++;
+    if (x == mone) return true;
+    if (x == one) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool prp_term(DevState *st, int64_t m, unsigned &tests, unsigned &sq) {
+  if ((uint64_t)m >= (1ull << 62)) {       // PrimeQ's domain (PrimeQ_x86.h:191)
+    atomicOr(&st->err_flags, ERR_DOMAIN);
+    return false;
+  }
+  tests++;
+  return sprp2((uint64_t)m, sq);
+}
+
+// ---- chain walk: checkn.cl:128-206 / cpuavx2.cpp:532-552 ------------------------
+__global__ void chain_kernel(ChainArgs A) {
+  const unsigned long long n_c = min(A.st->cand_count, (unsigned long long)A.cand_cap);
+  unsigned tests = 0, sq = 0;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_c;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const Cand cd = A.cand[i];
+    const int64_t S = A.jobs[cd.job].STEP;
+    const int64_t n = cd.n;
+    int k = 0;
+    int64_t m = n + S * 5;
+    while (prp_term(A.st, m, tests, sq)) { k++; m += S; }
+    if (k >= 10) {
+      m = n + S * 4;
+      while (m > 0 && prp_term(A.st, m, tests, sq)) { k++; m -= S; }
+    }
+    if (k >= 10) {
+      unsigned long long j = atomicAdd(&A.st->ap_count, 1ull);
+      if ((long long)j < A.ap_cap) {
+        A.aps[j].k = k;
+        A.aps[j].job = cd.job;
+        A.aps[j].first = m + S;
+        A.aps[j].n = n;
+      } else {
+        atomicOr(&A.st->err_flags, ERR_AP_OVERFLOW);
+      }
+    }
+  }
+  // warp-aggregated test counter
+  unsigned v = tests;
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&A.st->prp_tests, (unsigned long long)v);
+}
+
+}  // namespace ap26

@@ -1,0 +1,205 @@
+/* ap26.h -- C ABI of the B200-native AP26 per-K search (libap26.so).
+ *
+ * The search finds arithmetic progressions of primes first + j*K*23# with at
+ * least 10 base-2 strong-probable-prime terms, over the reference's 10-shift
+ * candidate set (SHIFT, SHIFT+64, ..., SHIFT+576), and reports each one raw,
+ * exactly as the reference's GPU kernel checkn (ibethune/ap26,
+ * src/opencl/kernels/checkn.cl:198-202) and CPU search
+ * (src/cpu/cpuavx2.cpp:548-552) hand it to ReportSolution.  Hashing,
+ * 9-base validation and SOL output stay on the host (ap26_report below),
+ * byte-compatible with src/common/AP26.cpp.
+ *
+ * Conventions: plain pointers and sizes; the caller owns every buffer; every
+ * entry point returns an int status (0 = AP26_OK, < 0 = error) and never
+ * exits the process; one host thread at a time per context.
+ */
+#ifndef AP26_H
+#define AP26_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define AP26_OK          0
+#define AP26_E_ARG      -1   /* bad argument / null pointer                  */
+#define AP26_E_CAPACITY -2   /* caller buffer too small; *n_out holds need   */
+#define AP26_E_CUDA     -3   /* CUDA runtime error                           */
+#define AP26_E_DOMAIN   -4   /* K / SHIFT outside the exact-arithmetic domain */
+#define AP26_E_TIMEOUT  -5   /* a bounded device wait gave up                */
+#define AP26_E_OVERFLOW -6   /* internal device buffer overflowed            */
+#define AP26_E_NOMEM    -7   /* device memory budget exceeded (admission)    */
+#define AP26_E_INVALID  -8   /* an AP failed even base-2 re-validation
+                                (reference: "Computation error", AP26.cpp:569-574) */
+#define AP26_E_NODEV    -9   /* no CUDA device / extension not usable        */
+
+/* Largest K for which the reference's int64 setup arithmetic
+ * (src/opencl/AP26.h:112-120) cannot overflow. */
+#define AP26_KMAX_SAFE 400000000
+/* Largest SHIFT such that every chain term stays below 2^62, the domain of
+ * the reference's PrimeQ (src/common/PrimeQ_x86.h:189-195). */
+#define AP26_SHIFT_MAX 16000
+
+/* ---- types -------------------------------------------------------------- */
+typedef struct ap26_ctx ap26_ctx;
+
+/* Tuning knobs; zero fields take the context's defaults (or autotuned values,
+ * see ap26_autotune). */
+typedef struct {
+  int32_t dense_primes;   /* primes sieved for all 10 words before compaction */
+  int32_t warp_queue;     /* per-warp shared-memory queue depth (items)       */
+  int32_t block_threads;  /* sieve CTA size (multiple of 32)                  */
+  int32_t chunk_tiles;    /* sieve tiles (256 n53 starts each) per launch     */
+  int32_t use_graphs;     /* 1 = capture per-chunk work in CUDA graphs        */
+  int32_t reserved;
+  int64_t mem_budget;     /* bytes of device memory the context may hold      */
+} ap26_opts;
+
+/* One raw report: AP length k, difference multiplier K, first term, and the
+ * sieve candidate n whose chain produced it (n orders reports the way the
+ * reference's AVX2 search meets them; see ap26_sort_aps). */
+typedef struct {
+  int32_t k;
+  int32_t K;
+  int64_t first;
+  int64_t n;
+} ap26_ap;
+
+typedef struct {
+  int64_t candidates;   /* sieve survivors after the 7..23 filter; the
+                           reference's "total n" (src/opencl/AP26.h:343)     */
+  int64_t late_items;   /* shift words that reached the late sieve stage     */
+  int64_t prp_tests;    /* base-2 SPRP tests run by the chain walk           */
+  int64_t aps;          /* raw reports (k >= 10)                             */
+  double device_ms;     /* CUDA-event time of the device work                */
+  int32_t error_flags;  /* bit 0: candidate buffer overflow (retried), bit 1:
+                           late buffer overflow (retried), bit 2: chain term
+                           >= 2^62, bit 3: AP buffer overflow                */
+  int32_t launches;     /* kernels launched for this call                    */
+} ap26_stats;
+
+/* A work item: every searchable K in [kmin, kmax] at one SHIFT. */
+typedef struct {
+  int64_t id;
+  int32_t kmin, kmax, shift, reserved;
+} ap26_item;
+
+typedef struct {
+  int64_t id;
+  int32_t status;       /* AP26_OK or an error code                          */
+  int32_t n_aps;        /* raw reports of this item                          */
+  int64_t first_ap;     /* index of its first report in the caller's array   */
+  int64_t candidates;   /* sieve survivors over all its K                    */
+  int32_t ks_searched;  /* K with will_search(K) true                        */
+  int32_t reserved;
+  double latency_ms;    /* serving: admission-to-completion wall time        */
+} ap26_item_result;
+
+/* ---- library / context --------------------------------------------------- */
+int ap26_version(void);
+const char *ap26_strerror(int code);
+/* Text of the last CUDA error / timeout seen by ctx ("" if none). */
+const char *ap26_last_error(const ap26_ctx *ctx);
+
+/* Creates a context on CUDA device `device` (replaces the OpenCL set-up and
+ * buffer allocation of src/common/AP26.cpp:834-939). */
+int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out);
+void ap26_destroy(ap26_ctx *ctx);
+int ap26_get_opts(const ap26_ctx *ctx, ap26_opts *out);
+
+/* ---- the per-K search (plain GPU form) -----------------------------------
+ * Replaces void SearchAP26(int K, int startSHIFT, int s_local, int compute)
+ * (src/opencl/AP26.h:78, called at src/common/AP26.cpp:976) and
+ * Search_avx2(K, SHIFT, ITER, K_COUNT, K_DONE) (src/cpu/cpuavx2.h:12).
+ * Writes the raw reports of K into out[0..cap), sorted in the reference's
+ * AVX2 order; *n_out = count.  The caller feeds them to ap26_report (or its
+ * own ReportSolution).  K must satisfy ap26_will_search(K). */
+int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int cap,
+                  int *n_out, ap26_stats *stats);
+
+/* ---- batched persistent form ----------------------------------------------
+ * All searchable K of all items in one persistent work-stealing pipeline:
+ * sieve tiles of every item share launches, survivors of every K share PRP
+ * batches.  Reports are grouped per item (res[i].first_ap, res[i].n_aps),
+ * inside an item by K ascending, inside a K in AVX2 order.  No counterpart
+ * in the reference: it replaces the per-K loop of AP26.cpp:957-982 when many
+ * workunits run in one process. */
+int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
+                      ap26_ap *aps, int64_t ap_cap, int64_t *n_aps,
+                      ap26_item_result *res, ap26_stats *stats);
+
+/* ---- serving: continuous batching ------------------------------------------
+ * Units are admitted while the device-memory budget allows (AP26_E_NOMEM
+ * otherwise); every ap26_serve_step runs one slice of sieve tiles drawn from
+ * all admitted units, so units submitted while others are on the GPU join the
+ * next slice.  Finished units are returned by ap26_serve_poll.  No
+ * counterpart in the reference (BOINC hands out one workunit per process). */
+int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item);
+int ap26_serve_step(ap26_ctx *ctx, int *active_units);
+int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *aps,
+                    int64_t ap_cap, int64_t *n_aps);
+
+/* ---- kernel-level entry points (parity and roofline measurements) -------- */
+/* Sieve only, over n53 starts [q_begin, q_end) of K (0 <= q < 137375320):
+ * candidate values n (unordered) into cand[0..cap); *n_cand = total.
+ * Replaces the sieve kernel (src/opencl/kernels/sieve.cl:218-362). */
+int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin,
+                     int64_t q_end, int64_t *cand, int64_t cap,
+                     int64_t *n_cand, ap26_stats *stats);
+/* Sieve survivor counts for nK values of K at one SHIFT (counts only). */
+int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int shift,
+                     int64_t *counts, ap26_stats *stats);
+/* Base-2 strong-PRP verdicts (1 = probable prime) for odd N in (2, 2^63).
+ * Replaces strong_prp (src/opencl/kernels/checkn.cl:59-122,
+ * src/common/PrimeQ_x86.h:143-182). */
+int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count,
+                    uint8_t *verdict, ap26_stats *stats);
+/* Chain walk for given candidates n of K (checkn.cl:128-206): k and first
+ * per candidate (first undefined when k < 10). */
+int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
+                     int32_t *k_out, int64_t *first_out, ap26_stats *stats);
+
+/* Picks dense_primes / warp_queue / block_threads / chunk_tiles by timing
+ * candidates on a fixed K sample, and stores them in the context. */
+int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen);
+
+/* Measured device peaks for the roofline: conflict-free shared-memory load
+ * bandwidth (GB/s) and 32-bit integer multiply-add throughput (Tops/s). */
+int ap26_probe_peaks(ap26_ctx *ctx, double *smem_gbs, double *int_tops);
+
+/* ---- host services (no GPU) -------------------------------------------------
+ * will_search: src/common/AP26.cpp:649-653. */
+int ap26_will_search(int K);
+
+/* ReportSolution (src/common/AP26.cpp:549-602): adds first%1000 + len to
+ * *result_hash (reduced by 2e9), re-validates with 9 SPRP bases, splits
+ * non-APs recursively, and appends "len K first\n" for valid APs with
+ * len >= 20 to sol[0..sol_cap) (NUL-terminated, *sol_len updated).
+ * Returns AP26_E_INVALID where the reference exits with "Computation
+ * error", AP26_E_CAPACITY if sol is too small. */
+int ap26_report(int32_t *result_hash, int len, int K, int64_t first,
+                char *sol, int sol_cap, int *sol_len);
+
+/* write_hash (AP26.cpp:295-357): 16 hex digits + NUL into out. */
+int ap26_hash_hex(int kmin, int kmax, int32_t result_hash, char *out17);
+
+/* Sorts reports of one K into the order the reference AVX2 search meets
+ * them (4-word passes, lattice order, word, bit: src/cpu/cpuavx2.cpp:334-820). */
+int ap26_sort_aps(ap26_ap *aps, int n, int shift);
+
+/* A/B checkpoint files (AP26.cpp:360-476) in directory dir ("" = cwd).
+ * write: alternates A/B as the reference does; read: returns 1 and fills
+ * *K, *ITER, *result_hash, *last_trickle if a matching state exists. */
+int ap26_write_state(const char *dir, int kmin, int kmax, int shift, int K,
+                     int ITER, int32_t result_hash, double last_trickle,
+                     int *write_a_next);
+int ap26_read_state(const char *dir, int kmin, int kmax, int shift, int *K,
+                    int *ITER, int32_t *result_hash, double *last_trickle,
+                    int *write_a_next);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AP26_H */
