@@ -33,8 +33,9 @@ PRIM23 = 223092870
 
 class Opts(ctypes.Structure):
     _fields_ = [("dense_primes", ctypes.c_int32), ("warp_queue", ctypes.c_int32),
-                ("block_threads", ctypes.c_int32), ("chunk_tiles", ctypes.c_int32),
-                ("use_graphs", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("block_threads", ctypes.c_int32), ("late_stage", ctypes.c_int32),
+                ("chunk_tiles", ctypes.c_int32), ("use_graphs", ctypes.c_int32),
+                ("profile", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("mem_budget", ctypes.c_int64)]
 
 
@@ -47,7 +48,9 @@ class Stats(ctypes.Structure):
     _fields_ = [("candidates", ctypes.c_int64), ("late_items", ctypes.c_int64),
                 ("prp_tests", ctypes.c_int64), ("aps", ctypes.c_int64),
                 ("device_ms", ctypes.c_double), ("error_flags", ctypes.c_int32),
-                ("launches", ctypes.c_int32)]
+                ("launches", ctypes.c_int32), ("sieve_ms", ctypes.c_double),
+                ("sieve_cells", ctypes.c_int64), ("sieve_launches", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -78,6 +81,8 @@ def _load():
         "ap26_create": (I, [I, P, P]),
         "ap26_destroy": (V, [P]),
         "ap26_get_opts": (I, [P, P]),
+        "ap26_set_opts": (I, [P, P]),
+        "ap26_list_variants": (I, [P, I]),
         "ap26_search_k": (I, [P, I, I, P, I, P, P]),
         "ap26_search_batch": (I, [P, P, I, P, I64, P, P, P]),
         "ap26_serve_submit": (I, [P, P]),
@@ -108,7 +113,7 @@ lib = _load()
 
 # Every symbol include/ap26.h declares (checked by the CPU test suite).
 EXPORTS = ("ap26_version", "ap26_strerror", "ap26_last_error", "ap26_create", "ap26_destroy",
-           "ap26_get_opts", "ap26_search_k", "ap26_search_batch", "ap26_serve_submit",
+           "ap26_get_opts", "ap26_set_opts", "ap26_list_variants", "ap26_search_k", "ap26_search_batch", "ap26_serve_submit",
            "ap26_serve_step", "ap26_serve_poll", "ap26_sieve_range", "ap26_sieve_count",
            "ap26_sprp_batch", "ap26_chain_batch", "ap26_autotune", "ap26_probe_peaks",
            "ap26_will_search",
@@ -175,6 +180,15 @@ def sort_aps(aps, shift):
     return [(a.k, a.K, a.first, a.n) for a in arr]
 
 
+def list_variants():
+    """Compiled sieve variants: [{dense_primes, warp_queue, block_threads, late_stage}]."""
+    n = lib.ap26_list_variants(None, 0)
+    arr = (Opts * n)()
+    lib.ap26_list_variants(arr, n)
+    return [{"dense_primes": o.dense_primes, "warp_queue": o.warp_queue,
+             "block_threads": o.block_threads, "late_stage": o.late_stage} for o in arr]
+
+
 def _aps_to_list(arr, n):
     return [(arr[i].k, arr[i].K, arr[i].first, arr[i].n) for i in range(n)]
 
@@ -218,6 +232,13 @@ class Context:
         o = Opts()
         self._check(lib.ap26_get_opts(self.h, ctypes.byref(o)), "ap26_get_opts")
         return {f: getattr(o, f) for f, _ in o._fields_}
+
+    def set_opts(self, **kw):
+        cur = self.opts
+        cur.update(kw)
+        o = Opts(**cur)
+        self._check(lib.ap26_set_opts(self.h, ctypes.byref(o)), "ap26_set_opts")
+        return self.opts
 
     def search_k(self, K, shift=0, cap=1 << 16):
         """Raw reports [(k, K, first, n)] of one K, AVX2 order, and stats."""

@@ -158,21 +158,27 @@ __global__ void chain_explicit_kernel(const KJob *job, const int64_t *n, long lo
 
 // ---- sieve variants (autotuner candidates) --------------------------------------
 struct SieveVariant {
-  int G, R, SL, QCAP, WARPS;
+  int G, R, SL, QCAP, LCAP, WARPS;
   void (*kernel)(SieveArgs);
-  size_t smem() const { return sizeof(uint4) * QCAP * WARPS + sizeof(uint32_t) * TABLE_WORDS; }
+  size_t smem() const {
+    return sizeof(uint4) * (QCAP + LCAP) * WARPS + sizeof(uint32_t) * TABLE_WORDS;
+  }
 };
 
-#define AP26_VARIANT(G, R, SL, Q, W) \
-  SieveVariant{G, R, SL, Q, W, sieve_kernel<G, R, SL, Q, W>}
+#define AP26_VARIANT(G, R, SL, Q, L, W) \
+  SieveVariant{G, R, SL, Q, L, W, sieve_kernel<G, R, SL, Q, L, W>}
 
+// (dense primes, tail group, late stage, queue, late queue, warps per CTA)
 static const SieveVariant kVariants[] = {
-    AP26_VARIANT(16, 4, 44, 448, 8),   // default
-    AP26_VARIANT(12, 4, 44, 448, 8),
-    AP26_VARIANT(20, 4, 44, 448, 8),
-    AP26_VARIANT(16, 4, 44, 640, 4),
-    AP26_VARIANT(16, 4, 36, 448, 8),
-    AP26_VARIANT(16, 4, 52, 448, 8),
+    AP26_VARIANT(16, 4, 44, 384, 128, 8),   // default
+    AP26_VARIANT(20, 4, 44, 384, 128, 8),
+    AP26_VARIANT(12, 4, 44, 384, 128, 8),
+    AP26_VARIANT(16, 4, 44, 384, 128, 4),
+    AP26_VARIANT(16, 4, 44, 512, 128, 8),
+    AP26_VARIANT(16, 4, 44, 640, 256, 4),
+    AP26_VARIANT(16, 4, 36, 384, 128, 8),
+    AP26_VARIANT(16, 4, 52, 384, 128, 8),
+    AP26_VARIANT(20, 4, 52, 384, 128, 8),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -219,6 +225,7 @@ struct ap26_ctx {
   // graphs
   cudaGraphExec_t chunk_graph = nullptr;
   long long graph_key = -1;
+  std::vector<cudaEvent_t> prof_events;   // per-sieve-launch timing pairs
   // serving
   std::deque<ServeUnit> units;
   std::deque<ServeUnit> finished;
@@ -262,21 +269,20 @@ static int default_opts(ap26_opts *o) {
   if (!o->dense_primes) o->dense_primes = kVariants[0].G;
   if (!o->warp_queue) o->warp_queue = kVariants[0].QCAP;
   if (!o->block_threads) o->block_threads = kVariants[0].WARPS * 32;
+  if (!o->late_stage) o->late_stage = kVariants[0].SL;
   if (!o->chunk_tiles) o->chunk_tiles = 32768;
   if (!o->mem_budget) o->mem_budget = (int64_t)8 << 30;
   return 0;
 }
 
-static int pick_variant(const ap26_opts &o, int sl_hint) {
-  int best = -1;
+static int pick_variant(const ap26_opts &o) {
   for (int i = 0; i < kNumVariants; i++) {
     const SieveVariant &v = kVariants[i];
     if (v.G == o.dense_primes && v.QCAP == o.warp_queue && v.WARPS * 32 == o.block_threads &&
-        (sl_hint <= 0 || v.SL == sl_hint)) {
-      if (best < 0 || v.SL == 44) best = i;
-    }
+        v.SL == o.late_stage)
+      return i;
   }
-  return best;
+  return -1;
 }
 
 static int set_variant(ap26_ctx *ctx, int vi) {
@@ -290,6 +296,7 @@ static int set_variant(ap26_ctx *ctx, int vi) {
   ctx->opts.dense_primes = v.G;
   ctx->opts.warp_queue = v.QCAP;
   ctx->opts.block_threads = v.WARPS * 32;
+  ctx->opts.late_stage = v.SL;
   if (ctx->chunk_graph) {
     cudaGraphExecDestroy(ctx->chunk_graph);
     ctx->chunk_graph = nullptr;
@@ -361,7 +368,7 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     CKC(cudaMallocHost(&ctx->h_st, sizeof(DevState)));
     CKC(cudaMallocHost(&ctx->h_aps, sizeof(APRec) * ctx->ap_cap));
     if ((rc = ensure_jobs(ctx, 64)) != AP26_OK) goto fail;
-    int vi = pick_variant(ctx->opts, 0);
+    int vi = pick_variant(ctx->opts);
     if (vi < 0) { rc = AP26_E_ARG; goto fail; }
     if ((rc = set_variant(ctx, vi)) != AP26_OK) goto fail;
   }
@@ -378,6 +385,7 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
+  for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
   cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
   cudaFree(ctx->d_st); cudaFree(ctx->d_cand); cudaFree(ctx->d_aps);
   cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts);
@@ -386,6 +394,39 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+
+extern "C" int ap26_list_variants(ap26_opts *out, int cap) {
+  for (int i = 0; i < kNumVariants && i < cap && out; i++) {
+    memset(&out[i], 0, sizeof(ap26_opts));
+    out[i].dense_primes = kVariants[i].G;
+    out[i].warp_queue = kVariants[i].QCAP;
+    out[i].block_threads = kVariants[i].WARPS * 32;
+    out[i].late_stage = kVariants[i].SL;
+  }
+  return kNumVariants;
+}
+
+extern "C" int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts) {
+  if (!ctx || !opts) return AP26_E_ARG;
+  ap26_opts o = ctx->opts;
+  if (opts->dense_primes) o.dense_primes = opts->dense_primes;
+  if (opts->warp_queue) o.warp_queue = opts->warp_queue;
+  if (opts->block_threads) o.block_threads = opts->block_threads;
+  if (opts->late_stage) o.late_stage = opts->late_stage;
+  if (opts->chunk_tiles) o.chunk_tiles = opts->chunk_tiles;
+  if (opts->mem_budget) o.mem_budget = opts->mem_budget;
+  o.use_graphs = opts->use_graphs;
+  o.profile = opts->profile;
+  const int vi = pick_variant(o);
+  if (vi < 0) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const int64_t keep_budget = o.mem_budget;
+  ctx->opts = o;
+  int rc = set_variant(ctx, vi);
+  ctx->opts.mem_budget = keep_budget;
+  if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
+  return rc;
 }
 
 extern "C" int ap26_get_opts(const ap26_ctx *ctx, ap26_opts *out) {
@@ -422,16 +463,17 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
                     long long *n_aps_out) {
   int rc;
   if ((rc = ensure_jobs(ctx, njobs)) != AP26_OK) return rc;
-  // tile prefix
+  // tile prefix; a tile is one start per thread of the variant's CTA
+  const SieveVariant &V = kVariants[ctx->variant];
+  const int64_t tile_n53 = (int64_t)V.WARPS * 32;
   unsigned long long tiles = 0;
   for (int j = 0; j < njobs; j++) {
     KJob &J = ctx->h_jobs[j];
     const int64_t span = J.q_end - J.q_begin;
-    J.ntiles = (int32_t)((span + TILE - 1) / TILE);
+    J.ntiles = (int32_t)((span + tile_n53 - 1) / tile_n53);
     J.tile_begin = (int64_t)tiles;
     tiles += (unsigned long long)J.ntiles;
   }
-  const SieveVariant &V = kVariants[ctx->variant];
   memset(ctx->h_st, 0, sizeof(DevState));
   ctx->h_st->chunk_size = (unsigned long long)ctx->opts.chunk_tiles;
   ctx->h_st->total_tiles = tiles;
@@ -469,12 +511,22 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaGraphInstantiate");
     ctx->graph_key = key;
   }
+  const bool prof = ctx->opts.profile != 0;
+  if (prof && (int)ctx->prof_events.size() < 2 * (int)nchunks) {
+    for (int i = (int)ctx->prof_events.size(); i < 2 * (int)nchunks; i++) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      ctx->prof_events.push_back(e);
+    }
+  }
   for (unsigned long long c = 0; c < nchunks; c++) {
-    if (use_graph) {
+    if (use_graph && !prof) {
       CK(cudaGraphLaunch(ctx->chunk_graph, s));
     } else {
       chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st);
+      if (prof) CK(cudaEventRecord(ctx->prof_events[2 * c], s));
       V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+      if (prof) CK(cudaEventRecord(ctx->prof_events[2 * c + 1], s));
       if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, s>>>(ca);
       chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap);
       CK(cudaGetLastError());
@@ -502,6 +554,19 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     stats->device_ms = ms;
     stats->error_flags = (int32_t)ctx->h_st->err_flags;
     stats->launches = launches;
+    int64_t n53 = 0;
+    for (int j = 0; j < njobs; j++) n53 += ctx->h_jobs[j].q_end - ctx->h_jobs[j].q_begin;
+    stats->sieve_cells = n53 * J59 * WORDS;
+    stats->sieve_launches = (int32_t)nchunks;
+    if (prof) {
+      double sm = 0;
+      for (unsigned long long c = 0; c < nchunks; c++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ctx->prof_events[2 * c], ctx->prof_events[2 * c + 1]);
+        sm += t;
+      }
+      stats->sieve_ms = sm;
+    }
   }
   if (count_only) {
     // count-only runs have no candidate buffer use: totals come from job counts
@@ -752,7 +817,8 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
   fill_job(ctx->h_jobs[0], K, shift, 0, q_begin, q_end);
   // sieve without the chain walk: one chunk covering everything, candidates kept
   const int saved = ctx->opts.chunk_tiles;
-  const int64_t tiles = (q_end - q_begin + TILE - 1) / TILE;
+  const int64_t tile_n53 = (int64_t)kVariants[ctx->variant].WARPS * 32;
+  const int64_t tiles = (q_end - q_begin + tile_n53 - 1) / tile_n53;
   ctx->opts.chunk_tiles = (int)std::max<int64_t>(1, tiles);
   if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
   const int saved_graph = ctx->opts.use_graphs;

@@ -8,7 +8,7 @@
 //                       per-K sieve bitstrings (replaces clearok/setok/
 //                       setupokok/offset, src/opencl/kernels/*.cl)
 //   chunk_begin_kernel  resets per-chunk counters
-//   sieve_kernel        persistent, work-stealing over 256-start tiles;
+//   sieve_kernel        persistent, work-stealing over tiles of n53 starts;
 //                       replaces setupn.cl + sieve.cl (the 1.1 GB n59 array
 //                       of the reference is never materialised: starts are
 //                       generated from a flat index)
@@ -34,9 +34,10 @@
 //   tail         live (n59, word) pairs are compacted into a per-warp shared
 //                queue (ballot/popc) and advanced R primes at a time, all
 //                lanes on the same prime, until stage SL
-//   late         the few pairs alive at SL finish lane-by-lane; surviving
-//                bits pass the 7..23 filter (sieve.cl:333-346) and become
-//                candidates n = n59 + (SHIFT + 64w + b) * MOD.
+//   late         pairs alive at SL wait in a second per-warp queue until
+//                enough have gathered to go through primes SL..82 together;
+//                surviving bits pass the 7..23 filter (sieve.cl:333-346) and
+//                become candidates n = n59 + (SHIFT + 64w + b) * MOD.
 #pragma once
 #include <stdint.h>
 #include <utility>
@@ -100,7 +101,7 @@ struct ChainArgs {
   long long ap_cap;
 };
 
-constexpr int TILE = 256;          // n53 starts per tile
+// A tile is one n53 start per thread of a sieve CTA: WARPS * 32 starts.
 constexpr uint32_t FULL = 0xffffffffu;
 
 // (i31, i37, i41) triples in the reference's loop order (AP26.h:127-131),
@@ -165,21 +166,6 @@ __device__ __forceinline__ void word_prime(const uint32_t *__restrict__ tab, uin
     lo &= __funnelshift_r(v0, v1, sh);
     hi &= __funnelshift_r(v1, v2, sh);
   }
-}
-
-// Same with runtime prime index (late stage; all active lanes share g).
-__device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab, int g,
-                                              uint32_t a, uint32_t b, uint32_t c,
-                                              uint32_t w64, uint32_t &lo, uint32_t &hi) {
-  const PrimeParam P = c_params[g];
-  uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
-  uint32_t s = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
-  uint32_t pos = s + w64;
-  const uint32_t *t = tab + P.off + (pos >> 5);
-  uint32_t sh = pos & 31;
-  uint32_t v0 = t[0], v1 = t[1], v2 = t[2];
-  lo &= __funnelshift_r(v0, v1, sh);
-  hi &= __funnelshift_r(v1, v2, sh);
 }
 
 // Queue item: x = n59 bits 0..31, y = n59 bits 32..47 | w << 16, z/w = mask.
@@ -254,30 +240,48 @@ __device__ __forceinline__ void tail_stages(const uint32_t *tab, uint4 *q, int &
   }
 }
 
-// Runs the queue to completion: stage-synchronous groups up to SL, then the
-// remaining items lane-by-lane through the last primes, then emission.
-template <int G, int R, int SL>
-__device__ __forceinline__ int drain_queue(const SieveArgs &A, const uint32_t *tab, uint4 *q,
-                                           int &cnt, int lane, int shift, int job,
-                                           unsigned long long &late) {
+// Per-warp late queue: items alive at stage SL wait there until 3/4 of its
+// LCAP slots are used, then go through the last primes together
+// (stage-synchronous, so the rare late items do not run lane-by-lane in
+// otherwise idle warps).
+
+// Late drain: primes SL..82 for every queued item, then emission of the
+// surviving bits of the fully sieved words.
+template <int R, int SL>
+__device__ __noinline__ int late_drain(const SieveArgs &A, const uint32_t *tab, uint4 *buf,
+                                          int &n, int lane, int shift, int job) {
+  tail_stages<SL, R, NPRIMES>(tab, buf, n, lane);
+  int kept = 0;
+  for (int i = lane; i < n; i += 32) {
+    const uint4 it = buf[i];
+    const uint64_t n59 = (uint64_t)it.x | ((uint64_t)(it.y & 0xffffu) << 32);
+    kept += emit_word(A, n59, (int)((it.y >> 16) & 15u), ((uint64_t)it.w << 32) | it.z, shift,
+                      job);
+  }
+  __syncwarp();
+  n = 0;
+  return kept;
+}
+
+// Front drain: stage-synchronous groups G..SL-1 over the main queue, then
+// the survivors move to the late queue (drained when it passes LTHRESH).
+template <int G, int R, int SL, int LCAP>
+__device__ __noinline__ int front_drain(const SieveArgs &A, const uint32_t *tab, uint4 *q,
+                                           int &cnt, uint4 *lq, int &lcnt, int lane, int shift,
+                                           int job, unsigned long long &late) {
   tail_stages<G, R, SL>(tab, q, cnt, lane);
   late += (unsigned long long)cnt;
   int kept = 0;
-  for (int i = lane; i < cnt; i += 32) {
-    uint4 it = q[i];
-    uint32_t a, b, c;
-    split_n59(it.x, it.y, a, b, c);
-    uint32_t wv = (it.y >> 16) & 15u;
-    uint32_t lo = it.z, hi = it.w;
-    for (int g = SL; g < NPRIMES && (lo | hi); g++)
-      word_prime_rt(tab, g, a, b, c, wv * 64u, lo, hi);
-    if (lo | hi) {
-      uint64_t n59 = (uint64_t)it.x | ((uint64_t)(it.y & 0xffffu) << 32);
-      kept += emit_word(A, n59, (int)wv, ((uint64_t)hi << 32) | lo, shift, job);
-    }
+  if (lcnt + cnt > LCAP) kept += late_drain<R, SL>(A, tab, lq, lcnt, lane, shift, job);
+  if (cnt > LCAP) {
+    kept += late_drain<R, SL>(A, tab, q, cnt, lane, shift, job);
+  } else {
+    for (int i = lane; i < cnt; i += 32) lq[lcnt + i] = q[i];
+    lcnt += cnt;
+    __syncwarp();
   }
-  __syncwarp();
   cnt = 0;
+  if (lcnt >= LCAP * 3 / 4) kept += late_drain<R, SL>(A, tab, lq, lcnt, lane, shift, job);
   return kept;
 }
 
@@ -320,14 +324,17 @@ __device__ __forceinline__ int find_job(const KJob *jobs, int njobs, unsigned lo
 }
 
 // ---- the sieve kernel -----------------------------------------------------------
-// Persistent: each CTA grabs 256-start tiles from DevState::tile_next until
-// the chunk window ends.  WARPS warps, one start per lane, 35 n59 per start.
-template <int G, int R, int SL, int QCAP, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
+// Persistent: each CTA grabs tiles (one n53 start per thread) from
+// DevState::tile_next until the chunk window ends; 35 n59 per start.  The
+// per-warp queues carry over from tile to tile and are flushed only when the
+// CTA moves to another K-job (the shared table changes) or runs out of work.
+template <int G, int R, int SL, int QCAP, int LCAP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 24 / WARPS)   // 24 resident warps per SM
 sieve_kernel(SieveArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
-  uint32_t *tab = reinterpret_cast<uint32_t *>(smem_raw + sizeof(uint4) * QCAP * WARPS);
+  uint4 *lqueues = queues + QCAP * WARPS;
+  uint32_t *tab = reinterpret_cast<uint32_t *>(lqueues + LCAP * WARPS);
   __shared__ unsigned long long s_tile;
   __shared__ int s_job;
   __shared__ unsigned long long s_kept[WARPS];
@@ -335,12 +342,15 @@ sieve_kernel(SieveArgs A) {
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint4 *q = queues + warp * QCAP;
-  constexpr int THRESH = QCAP - 32 * WORDS;
-  static_assert(THRESH >= 0, "queue too small for one dense batch");
+  uint4 *lq = lqueues + warp * LCAP;
+  // Drain once the queue holds THRESH items; a batch that would not fit is
+  // preceded by a drain, so QCAP only has to hold one worst-case batch.
+  constexpr int THRESH = QCAP - 128;
+  static_assert(QCAP >= 32 * WORDS, "queue too small for one dense batch");
 
-  int cur_job = -1;
+  int cur_job = -1, cur_shift = 0;
+  int cnt = 0, lcnt = 0;
   unsigned long long kept_acc = 0, late_acc = 0;
-  if (lane == 0) { s_kept[warp] = 0; s_late[warp] = 0; }
 
   for (;;) {
     if (threadIdx.x == 0) {
@@ -351,34 +361,38 @@ sieve_kernel(SieveArgs A) {
     __syncthreads();
     const unsigned long long tile = s_tile;
     const int job = s_job;
-    if (job < 0) break;
-    if (job != cur_job) {
-      // flush per-job survivor count of the previous job
+    // job < 0: the chunk window is exhausted (also on a CTA's first grab,
+    // when the chunk has fewer tiles than CTAs) -- flush and leave.
+    if (job != cur_job || job < 0) {
       if (cur_job >= 0) {
+        // finish the previous job's items with its table still in place
+        kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift,
+                                                cur_job, late_acc);
+        kept_acc += late_drain<R, SL>(A, tab, lq, lcnt, lane, cur_shift, cur_job);
         const unsigned long long v = warp_sum(kept_acc);
         if (lane == 0) s_kept[warp] = v;
+        kept_acc = 0;
         __syncthreads();
         if (threadIdx.x == 0) {
           unsigned long long s = 0;
           for (int i = 0; i < WARPS; i++) s += s_kept[i];
           if (s) atomicAdd(&A.job_counts[cur_job], s);
         }
-        kept_acc = 0;
       }
+      if (job < 0) break;
       const uint32_t *src = A.tables + (size_t)job * TABLE_WORDS;
       for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) tab[i] = src[i];
       cur_job = job;
+      cur_shift = A.jobs[job].shift;
       __syncthreads();
     }
     const KJob &J = A.jobs[job];
-    const int shift = J.shift;
     const int64_t S59 = J.S59;
-    int64_t qi = J.q_begin + (int64_t)(tile - (unsigned long long)J.tile_begin) * TILE +
-                 warp * 32 + lane;
+    const int64_t qi = J.q_begin +
+                       (int64_t)(tile - (unsigned long long)J.tile_begin) * (WARPS * 32) +
+                       warp * 32 + lane;
     const bool valid = qi < J.q_end;
     int64_t n59 = valid ? n53_at(J, qi) : 0;
-    int cnt = 0;
-    unsigned long long kept = 0;
 
     for (int j = 0; j < J59; j++) {
       uint32_t acc[20];
@@ -388,33 +402,37 @@ sieve_kernel(SieveArgs A) {
       uint32_t a, b, c;
       split_n59(x, y, a, b, c);
       dense_all(tab, a, b, c, acc, std::make_integer_sequence<int, G>{});
+      unsigned bal[WORDS];
+      int incoming = 0;
 #pragma unroll
       for (int w = 0; w < WORDS; w++) {
-        const uint32_t lo = acc[2 * w], hi = acc[2 * w + 1];
-        const bool live = (lo | hi) != 0u;
-        const unsigned bal = __ballot_sync(FULL, live);
-        if (live)
-          q[cnt + __popc(bal & ((1u << lane) - 1u))] =
-              make_uint4(x, y | ((uint32_t)w << 16), lo, hi);
-        cnt += __popc(bal);
+        bal[w] = __ballot_sync(FULL, (acc[2 * w] | acc[2 * w + 1]) != 0u);
+        incoming += __popc(bal[w]);
+      }
+      if (cnt + incoming > QCAP)
+        kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift, job,
+                                                late_acc);
+#pragma unroll
+      for (int w = 0; w < WORDS; w++) {
+        if ((bal[w] >> lane) & 1u)
+          q[cnt + __popc(bal[w] & ((1u << lane) - 1u))] =
+              make_uint4(x, y | ((uint32_t)w << 16), acc[2 * w], acc[2 * w + 1]);
+        cnt += __popc(bal[w]);
       }
       __syncwarp();
-      if (cnt > THRESH) kept += drain_queue<G, R, SL>(A, tab, q, cnt, lane, shift, job, late_acc);
+      if (cnt > THRESH)
+        kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift, job,
+                                                late_acc);
       n59 += S59;
       if (n59 >= MOD) n59 -= MOD;
     }
-    kept += drain_queue<G, R, SL>(A, tab, q, cnt, lane, shift, job, late_acc);
-    kept_acc += kept;
-    __syncthreads();   // all warps done with this tile's table before a reload
+    __syncthreads();   // the next grab overwrites s_tile / s_job
   }
-  // final flush (kept is per lane; late is warp-uniform)
-  const unsigned long long vk = warp_sum(kept_acc);
-  if (lane == 0) { s_kept[warp] = vk; s_late[warp] = late_acc; }
+  if (lane == 0) s_late[warp] = late_acc;   // warp-uniform
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long s = 0, l = 0;
-    for (int i = 0; i < WARPS; i++) { s += s_kept[i]; l += s_late[i]; }
-    if (cur_job >= 0 && s) atomicAdd(&A.job_counts[cur_job], s);
+    unsigned long long l = 0;
+    for (int i = 0; i < WARPS; i++) l += s_late[i];
     if (l) atomicAdd(&A.st->late_items, l);
   }
 }

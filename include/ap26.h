@@ -51,10 +51,15 @@ typedef struct {
   int32_t dense_primes;   /* primes sieved for all 10 words before compaction */
   int32_t warp_queue;     /* per-warp shared-memory queue depth (items)       */
   int32_t block_threads;  /* sieve CTA size (multiple of 32)                  */
-  int32_t chunk_tiles;    /* sieve tiles (256 n53 starts each) per launch     */
+  int32_t late_stage;     /* prime index where items move to the late queue   */
+  int32_t chunk_tiles;    /* sieve tiles (one n53 start per CTA thread) per
+                             launch                                           */
   int32_t use_graphs;     /* 1 = capture per-chunk work in CUDA graphs        */
+  int32_t profile;        /* 1 = time every sieve launch with CUDA events
+                             (ap26_stats.sieve_ms; disables graph replay)     */
   int32_t reserved;
-  int64_t mem_budget;     /* bytes of device memory the context may hold      */
+  int64_t mem_budget;     /* bytes of device memory held by admitted serving
+                             units (ap26_serve_submit)                        */
 } ap26_opts;
 
 /* One raw report: AP length k, difference multiplier K, first term, and the
@@ -78,6 +83,11 @@ typedef struct {
                            late buffer overflow (retried), bit 2: chain term
                            >= 2^62, bit 3: AP buffer overflow                */
   int32_t launches;     /* kernels launched for this call                    */
+  double sieve_ms;      /* summed CUDA-event time of the sieve launches
+                           (only with ap26_opts.profile = 1)                 */
+  int64_t sieve_cells;  /* (lattice value, shift word) cells sieved          */
+  int32_t sieve_launches;
+  int32_t reserved;
 } ap26_stats;
 
 /* A work item: every searchable K in [kmin, kmax] at one SHIFT. */
@@ -108,6 +118,14 @@ const char *ap26_last_error(const ap26_ctx *ctx);
 int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out);
 void ap26_destroy(ap26_ctx *ctx);
 int ap26_get_opts(const ap26_ctx *ctx, ap26_opts *out);
+/* Changes the options of a live context; the sieve variant is re-picked
+ * from (dense_primes, warp_queue, block_threads, late_stage), zero fields
+ * keep their current values.  AP26_E_ARG if no compiled variant matches. */
+int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts);
+/* The compiled sieve variants (autotuner search space): fills up to cap
+ * entries (dense_primes, warp_queue, block_threads, late_stage) and returns
+ * the total count. */
+int ap26_list_variants(ap26_opts *out, int cap);
 
 /* ---- the per-K search (plain GPU form) -----------------------------------
  * Replaces void SearchAP26(int K, int startSHIFT, int s_local, int compute)

@@ -22,7 +22,7 @@ if [ ! -f "$REF/src/common/AP26.cpp" ]; then
 fi
 mkdir -p "$OUT"
 CXX="${CXX:-g++}"
-CF="-O3 -m64 -DAP26_CPU -I$REF/src/cpu -I$REF/src/common"
+CF="-w -O3 -m64 -DAP26_CPU -I$REF/src/cpu -I$REF/src/common"
 $CXX $CF -c -o "$OUT/AP26.o"     "$REF/src/common/AP26.cpp"
 $CXX $CF -mavx2   -c -o "$OUT/cpuavx2.o"  "$REF/src/cpu/cpuavx2.cpp"
 $CXX $CF -mavx    -c -o "$OUT/cpuavx.o"   "$REF/src/cpu/cpuavx.cpp"

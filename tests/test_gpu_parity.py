@@ -81,6 +81,23 @@ def test_sieve_range_vs_oracle(ctx, oracle, K, shift, q0, q1):
     assert np.array_equal(np.sort(got), exp)
 
 
+@pytest.mark.parametrize("vi", range(len(A.list_variants())))
+def test_every_sieve_variant(ctx, oracle, vi):
+    """Every compiled variant (the autotuner's search space) is exact: a
+    ragged slice against the oracle and a whole K against the reference's
+    survivor known answer 38,838,420 (src/opencl/AP26.h:343)."""
+    variants = A.list_variants()
+    ctx.set_opts(**variants[vi])
+    try:
+        q0, q1 = 1000, 1000 + 3 * 12673 + 77
+        got, _ = ctx.sieve_range(366384, 0, q0, q1)
+        assert np.array_equal(np.sort(got), oracle_sieve(oracle, 366384, 0, q0, q1))
+        counts, _ = ctx.sieve_count([366384], 0)
+        assert counts[0] == 38838420
+    finally:
+        ctx.set_opts(**variants[0])
+
+
 def test_sieve_range_empty_and_single(ctx, oracle):
     got, _ = ctx.sieve_range(366384, 0, 100, 100)
     assert len(got) == 0
