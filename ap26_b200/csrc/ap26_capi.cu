@@ -161,7 +161,7 @@ struct SieveVariant {
   int G, R, SL, QCAP, LCAP, WARPS;
   void (*kernel)(SieveArgs);
   size_t smem() const {
-    return sizeof(uint4) * (QCAP + LCAP) * WARPS + sizeof(uint32_t) * TABLE_WORDS;
+    return sizeof(uint4) * (QCAP + LCAP) * WARPS + 2 * sizeof(uint32_t) * TABLE_WORDS;
   }
 };
 
@@ -170,15 +170,16 @@ struct SieveVariant {
 
 // (dense primes, tail group, late stage, queue, late queue, warps per CTA)
 static const SieveVariant kVariants[] = {
-    AP26_VARIANT(16, 4, 44, 384, 128, 8),   // default
+    AP26_VARIANT(20, 4, 44, 320, 96, 8),   // default
+    AP26_VARIANT(16, 4, 44, 320, 96, 8),
+    AP26_VARIANT(24, 4, 44, 320, 96, 8),
+    AP26_VARIANT(24, 4, 52, 320, 96, 8),
+    AP26_VARIANT(28, 4, 52, 320, 96, 8),
     AP26_VARIANT(20, 4, 44, 384, 128, 8),
-    AP26_VARIANT(12, 4, 44, 384, 128, 8),
-    AP26_VARIANT(16, 4, 44, 384, 128, 4),
-    AP26_VARIANT(16, 4, 44, 512, 128, 8),
-    AP26_VARIANT(16, 4, 44, 640, 256, 4),
-    AP26_VARIANT(16, 4, 36, 384, 128, 8),
-    AP26_VARIANT(16, 4, 52, 384, 128, 8),
-    AP26_VARIANT(20, 4, 52, 384, 128, 8),
+    AP26_VARIANT(24, 4, 52, 384, 128, 8),
+    AP26_VARIANT(20, 4, 44, 320, 96, 12),
+    AP26_VARIANT(24, 4, 52, 320, 96, 12),
+    AP26_VARIANT(20, 4, 44, 320, 96, 4),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 

@@ -130,42 +130,71 @@ __device__ __forceinline__ uint32_t window_start(uint32_t a, uint32_t b, uint32_
   return x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
 }
 
-// All 640 bits (20 words) of prime g ANDed into acc.
+// The shared table holds every bitstring twice: copy 0 at tab[0..), copy 1
+// (shifted down one word: copy1[i] = copy0[i+1]) at tab[TABLE_WORDS..).
+// Word w of a string is then the first half of an aligned 64-bit pair in
+// copy (w & 1), at index w & ~1.
+__device__ __forceinline__ const uint2 *pair_at(const uint32_t *tab, uint32_t off, uint32_t w) {
+  return reinterpret_cast<const uint2 *>(tab + (w & 1u) * TABLE_WORDS + off + (w & ~1u));
+}
+
+// All 640 bits (20 words) of prime g ANDed into acc: 11 pair loads, 20
+// funnel shifts.
 template <int g>
 __device__ __forceinline__ void dense_prime(const uint32_t *__restrict__ tab, uint32_t a,
                                             uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
   constexpr PrimeParam P = make_param(g);
-  uint32_t s = window_start<g>(a, b, c);
-  const uint32_t *t = tab + P.off + (s >> 5);
-  uint32_t sh = s & 31;
-  uint32_t v[21];
+  const uint32_t s = window_start<g>(a, b, c);
+  const uint2 *t = pair_at(tab, P.off, s >> 5);
+  const uint32_t sh = s & 31;
+  uint32_t v[22];
 #pragma unroll
-  for (int i = 0; i < 21; i++) v[i] = t[i];
+  for (int i = 0; i < 11; i++) {
+    const uint2 u = t[i];
+    v[2 * i] = u.x;
+    v[2 * i + 1] = u.y;
+  }
 #pragma unroll
   for (int i = 0; i < 20; i++) acc[i] &= __funnelshift_r(v[i], v[i + 1], sh);
 }
 
-template <int... I>
-__device__ __forceinline__ void dense_all(const uint32_t *tab, uint32_t a, uint32_t b,
-                                          uint32_t c, uint32_t (&acc)[20],
-                                          std::integer_sequence<int, I...>) {
-  (dense_prime<I>(tab, a, b, c, acc), ...);
+// Primes g and g+1 together: acc &= window_g & window_{g+1}, one 3-input
+// LOP3 per word instead of two ANDs.
+template <int g>
+__device__ __forceinline__ void dense_pair(const uint32_t *__restrict__ tab, uint32_t a,
+                                           uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
+  constexpr PrimeParam P = make_param(g), Q = make_param(g + 1);
+  const uint32_t s = window_start<g>(a, b, c), t = window_start<g + 1>(a, b, c);
+  const uint2 *tp = pair_at(tab, P.off, s >> 5);
+  const uint2 *tq = pair_at(tab, Q.off, t >> 5);
+  const uint32_t sp = s & 31, sq = t & 31;
+  uint32_t vp[22], vq[22];
+#pragma unroll
+  for (int i = 0; i < 11; i++) {
+    const uint2 u = tp[i], v = tq[i];
+    vp[2 * i] = u.x;
+    vp[2 * i + 1] = u.y;
+    vq[2 * i] = v.x;
+    vq[2 * i + 1] = v.y;
+  }
+#pragma unroll
+  for (int i = 0; i < 20; i++)
+    acc[i] &= __funnelshift_r(vp[i], vp[i + 1], sp) & __funnelshift_r(vq[i], vq[i + 1], sq);
 }
 
-// One word (64 bits starting at bit 64*w of the window) of prime g.
-template <int g>
-__device__ __forceinline__ void word_prime(const uint32_t *__restrict__ tab, uint32_t a,
-                                           uint32_t b, uint32_t c, uint32_t w64,
-                                           uint32_t &lo, uint32_t &hi) {
-  if constexpr (g < NPRIMES) {
-    constexpr PrimeParam P = make_param(g);
-    uint32_t pos = window_start<g>(a, b, c) + w64;
-    const uint32_t *t = tab + P.off + (pos >> 5);
-    uint32_t sh = pos & 31;
-    uint32_t v0 = t[0], v1 = t[1], v2 = t[2];
-    lo &= __funnelshift_r(v0, v1, sh);
-    hi &= __funnelshift_r(v1, v2, sh);
-  }
+template <int... I>
+__device__ __forceinline__ void dense_pairs(const uint32_t *tab, uint32_t a, uint32_t b,
+                                            uint32_t c, uint32_t (&acc)[20],
+                                            std::integer_sequence<int, I...>) {
+  (dense_pair<2 * I>(tab, a, b, c, acc), ...);
+}
+
+// The first G primes (G even) in pairs.
+template <int G>
+__device__ __forceinline__ void dense_all(const uint32_t *tab, uint32_t a, uint32_t b,
+                                          uint32_t c, uint32_t (&acc)[20]) {
+  static_assert(G % 2 == 0, "dense phase works on prime pairs");
+  dense_pairs(tab, a, b, c, acc, std::make_integer_sequence<int, G / 2>{});
 }
 
 // Queue item: x = n59 bits 0..31, y = n59 bits 32..47 | w << 16, z/w = mask.
@@ -201,42 +230,53 @@ __device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w
   return kept;
 }
 
-// Tail stage group: advance every queued item through primes g0..g0+R-1 and
-// compact the survivors in place (write index <= read index).
-template <int g0, int R>
-__device__ __forceinline__ void tail_group(const uint32_t *tab, uint4 *q, int &cnt, int lane) {
-  int out = 0;
-  for (int base = 0; base < cnt; base += 32) {
-    int i = base + lane;
-    bool valid = i < cnt;
-    uint4 it = valid ? q[i] : make_uint4(0, 0, 0, 0);
-    __syncwarp();
-    uint32_t a, b, c;
-    split_n59(it.x, it.y, a, b, c);
-    uint32_t w64 = ((it.y >> 16) & 15u) * 64u;
-    uint32_t lo = it.z, hi = it.w;
-    if constexpr (R > 0) word_prime<g0 + 0>(tab, a, b, c, w64, lo, hi);
-    if constexpr (R > 1) word_prime<g0 + 1>(tab, a, b, c, w64, lo, hi);
-    if constexpr (R > 2) word_prime<g0 + 2>(tab, a, b, c, w64, lo, hi);
-    if constexpr (R > 3) word_prime<g0 + 3>(tab, a, b, c, w64, lo, hi);
-    if constexpr (R > 4) word_prime<g0 + 4>(tab, a, b, c, w64, lo, hi);
-    if constexpr (R > 5) word_prime<g0 + 5>(tab, a, b, c, w64, lo, hi);
-    bool alive = valid && ((lo | hi) != 0u);
-    unsigned bal = __ballot_sync(FULL, alive);
-    if (alive) q[out + __popc(bal & ((1u << lane) - 1u))] = make_uint4(it.x, it.y, lo, hi);
-    out += __popc(bal);
-    __syncwarp();
-  }
-  cnt = out;
+// One word of prime P (runtime parameters, identical for all lanes).
+__device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
+                                              const PrimeParam &P, uint32_t a, uint32_t b,
+                                              uint32_t c, uint32_t w64, uint32_t &lo,
+                                              uint32_t &hi) {
+  const uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
+  const uint32_t pos = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k) + w64;
+  const uint32_t w = pos >> 5;
+  const uint2 u = *pair_at(tab, (uint32_t)P.off, w);
+  const uint32_t v2 = tab[P.off + w + 2];
+  const uint32_t sh = pos & 31;
+  lo &= __funnelshift_r(u.x, u.y, sh);
+  hi &= __funnelshift_r(u.y, v2, sh);
 }
 
-template <int g0, int R, int SL>
-__device__ __forceinline__ void tail_stages(const uint32_t *tab, uint4 *q, int &cnt, int lane) {
-  if constexpr (g0 < SL) {
-    if (cnt == 0) return;
-    constexpr int r = (g0 + R <= SL) ? R : (SL - g0);
-    tail_group<g0, r>(tab, q, cnt, lane);
-    tail_stages<g0 + r, R, SL>(tab, q, cnt, lane);
+// Tail stages g_begin..g_end-1: every queued item advances R primes per pass
+// (all lanes on the same primes, read warp-uniformly from constant memory),
+// then the survivors are compacted in place (write index <= read index).
+// One copy of this code serves every stage of both queues.
+template <int R>
+__device__ __forceinline__ void tail_stages(const uint32_t *tab, uint4 *q, int &cnt, int lane,
+                                            int g_begin, int g_end) {
+  for (int g0 = g_begin; g0 < g_end && cnt > 0; g0 += R) {
+    PrimeParam P[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) P[r] = c_params[min(g0 + r, NPRIMES - 1)];
+    const int nr = min(R, g_end - g0);
+    int out = 0;
+    for (int base = 0; base < cnt; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < cnt;
+      const uint4 it = valid ? q[i] : make_uint4(0, 0, 0, 0);
+      __syncwarp();
+      uint32_t a, b, c;
+      split_n59(it.x, it.y, a, b, c);
+      const uint32_t w64 = ((it.y >> 16) & 15u) * 64u;
+      uint32_t lo = it.z, hi = it.w;
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (r < nr) word_prime_rt(tab, P[r], a, b, c, w64, lo, hi);
+      const bool alive = valid && ((lo | hi) != 0u);
+      const unsigned bal = __ballot_sync(FULL, alive);
+      if (alive) q[out + __popc(bal & ((1u << lane) - 1u))] = make_uint4(it.x, it.y, lo, hi);
+      out += __popc(bal);
+      __syncwarp();
+    }
+    cnt = out;
   }
 }
 
@@ -248,9 +288,9 @@ __device__ __forceinline__ void tail_stages(const uint32_t *tab, uint4 *q, int &
 // Late drain: primes SL..82 for every queued item, then emission of the
 // surviving bits of the fully sieved words.
 template <int R, int SL>
-__device__ __noinline__ int late_drain(const SieveArgs &A, const uint32_t *tab, uint4 *buf,
+__device__ __forceinline__ int late_drain(const SieveArgs &A, const uint32_t *tab, uint4 *buf,
                                           int &n, int lane, int shift, int job) {
-  tail_stages<SL, R, NPRIMES>(tab, buf, n, lane);
+  tail_stages<R>(tab, buf, n, lane, SL, NPRIMES);
   int kept = 0;
   for (int i = lane; i < n; i += 32) {
     const uint4 it = buf[i];
@@ -264,24 +304,30 @@ __device__ __noinline__ int late_drain(const SieveArgs &A, const uint32_t *tab, 
 }
 
 // Front drain: stage-synchronous groups G..SL-1 over the main queue, then
-// the survivors move to the late queue (drained when it passes LTHRESH).
+// the survivors move to the late queue (drained when it passes 3/4 full).
+// With force, the late queue is drained too (job change / end of work).
+// The late queue is drained at a single call site: moving items in, it is
+// drained whenever it fills, and finally once it passes 3/4 of LCAP.
 template <int G, int R, int SL, int LCAP>
-__device__ __noinline__ int front_drain(const SieveArgs &A, const uint32_t *tab, uint4 *q,
+__device__ __forceinline__ int front_drain(const SieveArgs &A, const uint32_t *tab, uint4 *q,
                                            int &cnt, uint4 *lq, int &lcnt, int lane, int shift,
-                                           int job, unsigned long long &late) {
-  tail_stages<G, R, SL>(tab, q, cnt, lane);
+                                           int job, unsigned long long &late, bool force) {
+  tail_stages<R>(tab, q, cnt, lane, G, SL);
   late += (unsigned long long)cnt;
   int kept = 0;
-  if (lcnt + cnt > LCAP) kept += late_drain<R, SL>(A, tab, lq, lcnt, lane, shift, job);
-  if (cnt > LCAP) {
-    kept += late_drain<R, SL>(A, tab, q, cnt, lane, shift, job);
-  } else {
-    for (int i = lane; i < cnt; i += 32) lq[lcnt + i] = q[i];
-    lcnt += cnt;
+  int moved = 0;
+  for (;;) {
+    const int take = min(LCAP - lcnt, cnt - moved);
+    for (int i = lane; i < take; i += 32) lq[lcnt + i] = q[moved + i];
+    lcnt += take;
+    moved += take;
     __syncwarp();
+    const bool more = moved < cnt;
+    if (more || lcnt >= LCAP * 3 / 4 || (force && lcnt > 0))
+      kept += late_drain<R, SL>(A, tab, lq, lcnt, lane, shift, job);
+    if (!more) break;
   }
   cnt = 0;
-  if (lcnt >= LCAP * 3 / 4) kept += late_drain<R, SL>(A, tab, lq, lcnt, lane, shift, job);
   return kept;
 }
 
@@ -343,9 +389,8 @@ sieve_kernel(SieveArgs A) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint4 *q = queues + warp * QCAP;
   uint4 *lq = lqueues + warp * LCAP;
-  // Drain once the queue holds THRESH items; a batch that would not fit is
-  // preceded by a drain, so QCAP only has to hold one worst-case batch.
-  constexpr int THRESH = QCAP - 128;
+  // The queue is drained when the next dense batch would not fit, so QCAP
+  // only has to hold one worst-case batch and drains run on a full queue.
   static_assert(QCAP >= 32 * WORDS, "queue too small for one dense batch");
 
   int cur_job = -1, cur_shift = 0;
@@ -367,8 +412,7 @@ sieve_kernel(SieveArgs A) {
       if (cur_job >= 0) {
         // finish the previous job's items with its table still in place
         kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift,
-                                                cur_job, late_acc);
-        kept_acc += late_drain<R, SL>(A, tab, lq, lcnt, lane, cur_shift, cur_job);
+                                                cur_job, late_acc, true);
         const unsigned long long v = warp_sum(kept_acc);
         if (lane == 0) s_kept[warp] = v;
         kept_acc = 0;
@@ -381,7 +425,10 @@ sieve_kernel(SieveArgs A) {
       }
       if (job < 0) break;
       const uint32_t *src = A.tables + (size_t)job * TABLE_WORDS;
-      for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) tab[i] = src[i];
+      for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) {
+        tab[i] = src[i];
+        tab[TABLE_WORDS + i] = (i + 1 < TABLE_WORDS) ? src[i + 1] : 0u;
+      }
       cur_job = job;
       cur_shift = A.jobs[job].shift;
       __syncthreads();
@@ -401,7 +448,7 @@ sieve_kernel(SieveArgs A) {
       const uint32_t x = (uint32_t)n59, y = (uint32_t)((uint64_t)n59 >> 32);
       uint32_t a, b, c;
       split_n59(x, y, a, b, c);
-      dense_all(tab, a, b, c, acc, std::make_integer_sequence<int, G>{});
+      dense_all<G>(tab, a, b, c, acc);
       unsigned bal[WORDS];
       int incoming = 0;
 #pragma unroll
@@ -411,7 +458,7 @@ sieve_kernel(SieveArgs A) {
       }
       if (cnt + incoming > QCAP)
         kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift, job,
-                                                late_acc);
+                                                late_acc, false);
 #pragma unroll
       for (int w = 0; w < WORDS; w++) {
         if ((bal[w] >> lane) & 1u)
@@ -420,9 +467,6 @@ sieve_kernel(SieveArgs A) {
         cnt += __popc(bal[w]);
       }
       __syncwarp();
-      if (cnt > THRESH)
-        kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift, job,
-                                                late_acc);
       n59 += S59;
       if (n59 >= MOD) n59 -= MOD;
     }
