@@ -231,6 +231,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     import ap26_b200 as A
+    from ap26_b200 import replicas
 
     ctx = A.Context(local, profile=1)
     tuned = None
@@ -238,7 +239,7 @@ def main():
         tuned = ctx.autotune(KMIN_SEEDED + 64 * rank if will_search(KMIN_SEEDED + 64 * rank)
                              else KMIN_SEEDED)
     smem_gbs, int_tops = ctx.probe_peaks()
-    kmin = KMIN_SEEDED + RANGE_K * rank
+    kmin, _ = replicas.rank_range(KMIN_SEEDED, RANGE_K, rank)
     nsteps_range = RANGE_K // STEP_K
 
     def step_items(i):

@@ -1,0 +1,59 @@
+"""The ap26 command (the reference's CLI contract, src/common/AP26.cpp:660-1041)
+on the GPU: golden SOL file, A/B checkpoint files, resume after a stop
+between K, and the batched form writing the same output."""
+import os
+import subprocess
+
+import pytest
+
+from conftest import golden_sol, ref_raw
+
+import ap26_b200 as A
+
+pytestmark = pytest.mark.gpu
+
+
+def run_cli(cwd, *args):
+    p = subprocess.run([A.CLI_PATH] + [str(a) for a in args], cwd=cwd, capture_output=True,
+                       text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    return p
+
+
+def test_cli_reproduces_golden_sol_and_final_state(tmp_path):
+    run_cli(tmp_path, 366384, 366384, 0)
+    assert (tmp_path / "SOL-AP26.txt").read_text() == golden_sol(366384)
+    # checkpoint before the K (state A), final one with K = KMAX+1 (state B)
+    a = (tmp_path / "AP26-state.a.txt").read_text().split()
+    b = (tmp_path / "AP26-state.b.txt").read_text().split()
+    assert a[:6] == ["366384", "366384", "0", "366384", "0", "0"]
+    assert b[:6] == ["366384", "366384", "0", "366385", "0", "87376"]
+
+
+def test_cli_resume_equals_uninterrupted_run(tmp_path):
+    kmin, kmax = 366384, 366386        # 366385 is searchable; 366386 = 29 * 12634 is skipped
+    full = tmp_path / "full"
+    full.mkdir()
+    run_cli(full, kmin, kmax, 0)
+    expected = (full / "SOL-AP26.txt").read_text()
+    # a run stopped after its first K: the checkpoint written before K=366385
+    # holds K=366385 and the hash of K=366384 (87376), as the reference writes
+    part = tmp_path / "resumed"
+    part.mkdir()
+    r = A.Reporter()
+    r.report_all(ref_raw(366384))
+    (part / "AP26-state.a.txt").write_text(f"{kmin} {kmax} 0 366385 0 {r.hash.value} 0.000000\n")
+    (part / "SOL-AP26.txt").write_text("".join(l + "\n" for l in r.sol))
+    p = run_cli(part, kmin, kmax, 0)
+    assert "Resuming" in p.stdout
+    assert (part / "SOL-AP26.txt").read_text() == expected
+
+
+def test_cli_batched_form_writes_same_output(tmp_path):
+    a = tmp_path / "plain"
+    b = tmp_path / "batched"
+    a.mkdir()
+    b.mkdir()
+    run_cli(a, 1000037, 1000041, 640)
+    run_cli(b, 1000037, 1000041, 640, "-batch", 3)
+    assert (a / "SOL-AP26.txt").read_text() == (b / "SOL-AP26.txt").read_text()
