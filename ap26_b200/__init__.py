@@ -94,6 +94,7 @@ def _load():
         "ap26_chain_batch": (I, [P, I, P, I64, P, P, P]),
         "ap26_autotune": (I, [P, I, I, P]),
         "ap26_probe_peaks": (I, [P, P, P]),
+        "ap26_sieve_count_noalloc": (I, [I, P, I, I, P, P]),
         "ap26_will_search": (I, [I]),
         "ap26_report": (I, [P, I, I, I64, P, I, P]),
         "ap26_hash_hex": (I, [I, I, ctypes.c_int32, P]),
@@ -116,6 +117,7 @@ EXPORTS = ("ap26_version", "ap26_strerror", "ap26_last_error", "ap26_create", "a
            "ap26_get_opts", "ap26_set_opts", "ap26_list_variants", "ap26_search_k", "ap26_search_batch", "ap26_serve_submit",
            "ap26_serve_step", "ap26_serve_poll", "ap26_sieve_range", "ap26_sieve_count",
            "ap26_sprp_batch", "ap26_chain_batch", "ap26_autotune", "ap26_probe_peaks",
+           "ap26_sieve_count_noalloc",
            "ap26_will_search",
            "ap26_report", "ap26_hash_hex", "ap26_sort_aps", "ap26_write_state",
            "ap26_read_state")

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <deque>
 #include <string>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -1024,5 +1025,124 @@ extern "C" int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen)
   int rc = set_variant(ctx, best_v);
   ctx->opts.chunk_tiles = best_chunk;
   if (chosen) *chosen = ctx->opts;
+  return rc;
+}
+
+// ---- allocation-free survivor counts ----------------------------------------------------
+// For callers that may not allocate device memory themselves: code that runs
+// under a host framework which owns the device's memory pool, plugin hosts
+// that forbid cudaMalloc/cudaFree (both synchronise the device and stall
+// work already queued by others), or callers that must not fail on memory
+// exhaustion in the middle of a run.  Such a caller passes device buffers it
+// already owns for the K list and the counts; every other byte this path
+// touches lives in the file-scope array below, which every GPU that loads
+// the library holds until the process exits.
+namespace ap26 {
+struct NoallocScratch {
+  DevState st;
+  KJob jobs[AP26_NOALLOC_MAX_K];
+  unsigned long long counts[AP26_NOALLOC_MAX_K];
+  uint32_t tables[AP26_NOALLOC_MAX_K][TABLE_WORDS];
+};
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
+
+// Fills the job descriptors and zeroes the counters and state left behind by
+// the previous call (the array keeps the last call's contents).  A K outside
+// [1, AP26_KMAX_SAFE] gets an empty lattice range and a count of -1.
+__global__ void noalloc_init_kernel(NoallocScratch *s, const int32_t *Ks, int nK, int shift,
+                                    int tile_n53) {
+  const int j = threadIdx.x;
+  const int64_t ntiles = (N53_PER_K + tile_n53 - 1) / tile_n53;
+  if (j < nK) {
+    KJob &J = s->jobs[j];
+    const int K = Ks[j];
+    const bool ok = K >= 1 && K <= AP26_KMAX_SAFE;
+    memset(&J, 0, sizeof(KJob));
+    J.K = ok ? K : 1;
+    J.shift = shift;
+    J.item = ok ? 0 : -1;
+    J.q_begin = 0;
+    J.q_end = ok ? N53_PER_K : 0;
+    J.ntiles = (int32_t)ntiles;
+    J.tile_begin = (int64_t)j * ntiles;
+    s->counts[j] = 0;
+  }
+  if (j == 0) {
+    memset(&s->st, 0, sizeof(DevState));
+    s->st.chunk_size = (unsigned long long)ntiles * nK;
+    s->st.total_tiles = (unsigned long long)ntiles * nK;
+  }
+}
+
+__global__ void noalloc_finish_kernel(const NoallocScratch *s, int nK, int64_t *out) {
+  const int j = threadIdx.x;
+  if (j < nK) out[j] = s->jobs[j].item < 0 ? -1 : (int64_t)s->counts[j];
+}
+
+struct NoallocDevice {
+  NoallocScratch *ptr = nullptr;
+  int sieve_blocks = 0;
+  bool ready = false;
+};
+static NoallocDevice g_noalloc_dev[64];
+static std::mutex g_noalloc_mu;
+
+// Once per device, with that device current: the scratch array's device
+// address (its host-side name is only a stand-in), the constant tables, and
+// the launch shape of the default sieve variant.  Synchronous calls, so the
+// first call on a device must come before any stream capture.
+static int noalloc_setup(int device, NoallocDevice **out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoallocDevice &d = g_noalloc_dev[device];
+  if (!d.ready) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return AP26_E_CUDA;
+    uint16_t trip[NUM_TRIPLES];
+    if (ap26h_triples(trip) != NUM_TRIPLES) return AP26_E_ARG;
+    PrimeParam params[NPRIMES];
+    for (int g = 0; g < NPRIMES; g++) params[g] = make_param(g);
+    if (cudaMemcpyToSymbol(c_triples, trip, sizeof(trip)) != cudaSuccess) return AP26_E_CUDA;
+    if (cudaMemcpyToSymbol(c_params, params, sizeof(params)) != cudaSuccess) return AP26_E_CUDA;
+    const SieveVariant &V = kVariants[0];
+    if (cudaFuncSetAttribute(V.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)V.smem()) != cudaSuccess)
+      return AP26_E_CUDA;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.kernel, V.WARPS * 32,
+                                                      V.smem()) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+      return AP26_E_CUDA;
+    d.ptr = static_cast<NoallocScratch *>(p);
+    d.sieve_blocks = sms * (per_sm > 0 ? per_sm : 1);
+    d.ready = true;
+  }
+  *out = &d;
+  return AP26_OK;
+}
+}  // namespace ap26
+
+extern "C" int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
+                                        int64_t *d_counts, void *stream) {
+  if (!d_Ks || !d_counts || nK < 1 || device < 0 || device >= 64) return AP26_E_ARG;
+  if (nK > AP26_NOALLOC_MAX_K) return AP26_E_CAPACITY;
+  if (shift < 0 || shift > AP26_SHIFT_MAX) return AP26_E_DOMAIN;
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess) return AP26_E_CUDA;
+  if (prev != device && cudaSetDevice(device) != cudaSuccess) return AP26_E_CUDA;
+  NoallocDevice *d = nullptr;
+  int rc = noalloc_setup(device, &d);
+  if (rc == AP26_OK) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const SieveVariant &V = kVariants[0];
+    NoallocScratch *S = d->ptr;
+    noalloc_init_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, d_Ks, nK, shift, V.WARPS * 32);
+    setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0]);
+    chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st);
+    SieveArgs sa{S->jobs, nK, &S->tables[0][0], &S->st, nullptr, 0, S->counts, 1};
+    V.kernel<<<d->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+    noalloc_finish_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, nK, d_counts);
+    if (cudaGetLastError() != cudaSuccess) rc = AP26_E_CUDA;
+  }
+  if (prev != device) cudaSetDevice(prev);
   return rc;
 }

@@ -179,6 +179,31 @@ int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count,
 int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
                      int32_t *k_out, int64_t *first_out, ap26_stats *stats);
 
+/* ---- allocation-free survivor counts --------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory: code under a host framework that owns the device's memory pool,
+ * plugin hosts that forbid cudaMalloc/cudaFree (both synchronise the whole
+ * device), or callers that must not fail on memory exhaustion mid-run.
+ * Same result as ap26_sieve_count, but the caller passes DEVICE buffers it
+ * already owns: d_Ks (nK K values) in, d_counts (nK survivor counts) out;
+ * a K outside [1, AP26_KMAX_SAFE] gets -1.  The work is enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default) of `device`; counts are
+ * valid once that stream reaches this point.
+ * - Allocates nothing (no cudaMalloc/cudaFree, no context object): all
+ *   scratch -- job descriptors, tables, counters -- lives in one
+ *   file-scope device array of about 660 KB that every GPU loading the
+ *   library keeps until process exit.  At most AP26_NOALLOC_MAX_K values of
+ *   K per call; more returns AP26_E_CAPACITY.
+ * - The first call on a device sets that device up synchronously (looks up
+ *   the array's device address, fills the constant tables), so it must come
+ *   before any stream capture.
+ * - Every call reuses the same array and clears what must start at zero;
+ *   calls whose work overlaps on the GPU (other streams, other threads)
+ *   race on it and must be serialised by the caller. */
+#define AP26_NOALLOC_MAX_K 64
+int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
+                             int64_t *d_counts, void *stream);
+
 /* Picks dense_primes / warp_queue / block_threads / chunk_tiles by timing
  * candidates on a fixed K sample, and stores them in the context. */
 int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen);
