@@ -78,15 +78,16 @@ __global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables) {
   }
 }
 
-__global__ void chunk_begin_kernel(DevState *st) {
+// Chunk bookkeeping; `ring` selects the candidate ring this chunk fills.
+__global__ void chunk_begin_kernel(DevState *st, int ring) {
   st->tile_next = st->chunk_begin;
   unsigned long long e = st->chunk_begin + st->chunk_size;
   st->tile_end = e < st->total_tiles ? e : st->total_tiles;
-  st->cand_count = 0;
+  st->cand_count[ring] = 0;
 }
 
-__global__ void chunk_end_kernel(DevState *st, long long cand_cap) {
-  unsigned long long c = st->cand_count;
+__global__ void chunk_end_kernel(DevState *st, long long cand_cap, int ring) {
+  unsigned long long c = st->cand_count[ring];
   st->cand_total += c;
   if ((long long)c > cand_cap) st->err_flags |= ERR_CAND_OVERFLOW;
   st->chunk_begin += st->chunk_size;
@@ -157,6 +158,37 @@ __global__ void chain_explicit_kernel(const KJob *job, const int64_t *n, long lo
   }
 }
 
+// Argument blocks are only built through these, so no field can be left
+// value-initialised (a null counter pointer would fault on the device).
+static SieveArgs sieve_args(const KJob *jobs, int njobs, const uint32_t *tables, DevState *st,
+                            Cand *cand, long long cand_cap, unsigned long long *job_counts,
+                            int count_only, unsigned long long *cand_count) {
+  SieveArgs a;
+  a.jobs = jobs;
+  a.njobs = njobs;
+  a.tables = tables;
+  a.st = st;
+  a.cand = cand;
+  a.cand_cap = cand_cap;
+  a.job_counts = job_counts;
+  a.count_only = count_only;
+  a.cand_count = cand_count;
+  return a;
+}
+
+static ChainArgs chain_args(const KJob *jobs, DevState *st, const Cand *cand, long long cand_cap,
+                            APRec *aps, long long ap_cap, const unsigned long long *cand_count) {
+  ChainArgs a;
+  a.jobs = jobs;
+  a.st = st;
+  a.cand = cand;
+  a.cand_cap = cand_cap;
+  a.aps = aps;
+  a.ap_cap = ap_cap;
+  a.cand_count = cand_count;
+  return a;
+}
+
 // ---- sieve variants (autotuner candidates) --------------------------------------
 struct SieveVariant {
   int G, R, SL, QCAP, LCAP, WARPS;
@@ -207,6 +239,8 @@ struct ap26_ctx {
   ap26_opts opts{};
   int variant = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;              // chain walks of the overlapped form
+  cudaEvent_t sieve_done[2] = {nullptr, nullptr}, chain_done[2] = {nullptr, nullptr};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 0, sieve_blocks = 0, chain_blocks = 0;
   // device buffers
@@ -215,7 +249,7 @@ struct ap26_ctx {
   unsigned long long *d_job_counts = nullptr;
   int jobs_cap = 0;
   DevState *d_st = nullptr;
-  Cand *d_cand = nullptr;
+  Cand *d_cand[2] = {nullptr, nullptr};   // two candidate rings (overlapped form)
   long long cand_cap = 0;
   APRec *d_aps = nullptr;
   long long ap_cap = 0;
@@ -365,7 +399,13 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     ctx->cand_cap = 8ll << 20;
     ctx->ap_cap = 1ll << 20;
     CKC(cudaMalloc(&ctx->d_st, sizeof(DevState)));
-    CKC(cudaMalloc(&ctx->d_cand, sizeof(Cand) * ctx->cand_cap));
+    CKC(cudaMalloc(&ctx->d_cand[0], sizeof(Cand) * ctx->cand_cap));
+    CKC(cudaMalloc(&ctx->d_cand[1], sizeof(Cand) * ctx->cand_cap));
+    CKC(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+    for (int r = 0; r < 2; r++) {
+      CKC(cudaEventCreateWithFlags(&ctx->sieve_done[r], cudaEventDisableTiming));
+      CKC(cudaEventCreateWithFlags(&ctx->chain_done[r], cudaEventDisableTiming));
+    }
     CKC(cudaMalloc(&ctx->d_aps, sizeof(APRec) * ctx->ap_cap));
     CKC(cudaMallocHost(&ctx->h_st, sizeof(DevState)));
     CKC(cudaMallocHost(&ctx->h_aps, sizeof(APRec) * ctx->ap_cap));
@@ -389,7 +429,12 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
   for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
   cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
-  cudaFree(ctx->d_st); cudaFree(ctx->d_cand); cudaFree(ctx->d_aps);
+  cudaFree(ctx->d_st); cudaFree(ctx->d_cand[0]); cudaFree(ctx->d_cand[1]); cudaFree(ctx->d_aps);
+  for (int r = 0; r < 2; r++) {
+    if (ctx->sieve_done[r]) cudaEventDestroy(ctx->sieve_done[r]);
+    if (ctx->chain_done[r]) cudaEventDestroy(ctx->chain_done[r]);
+  }
+  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts);
   cudaFreeHost(ctx->h_st); cudaFreeHost(ctx->h_aps);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -462,7 +507,7 @@ static int wait_stream(ap26_ctx *ctx, double timeout_s) {
 // and item filled by the caller).  count_only: survivors are counted, no
 // chain walk.  Returns after the D2H of state, counts and reports.
 static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
-                    long long *n_aps_out) {
+                    long long *n_aps_out, bool overlap = false) {
   int rc;
   if ((rc = ensure_jobs(ctx, njobs)) != AP26_OK) return rc;
   // tile prefix; a tile is one start per thread of the variant's CTA
@@ -487,12 +532,22 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
   setup_jobs_kernel<<<njobs, 256, 0, s>>>(ctx->d_jobs, njobs, ctx->d_tables);
   CK(cudaGetLastError());
   int launches = 1;
-  SieveArgs sa{ctx->d_jobs, njobs, ctx->d_tables, ctx->d_st, ctx->d_cand, ctx->cand_cap,
-               ctx->d_job_counts, count_only ? 1 : 0};
-  ChainArgs ca{ctx->d_jobs, ctx->d_st, ctx->d_cand, ctx->cand_cap, ctx->d_aps, ctx->ap_cap};
+  // ring r: candidate buffer d_cand[r] and its fill count DevState::cand_count[r]
+  SieveArgs sa[2];
+  ChainArgs ca[2];
+  for (int r = 0; r < 2; r++) {
+    sa[r] = sieve_args(ctx->d_jobs, njobs, ctx->d_tables, ctx->d_st, ctx->d_cand[r],
+                       ctx->cand_cap, ctx->d_job_counts, count_only ? 1 : 0,
+                       &ctx->d_st->cand_count[r]);
+    ca[r] = chain_args(ctx->d_jobs, ctx->d_st, ctx->d_cand[r], ctx->cand_cap, ctx->d_aps,
+                       ctx->ap_cap, &ctx->d_st->cand_count[r]);
+  }
   const unsigned long long nchunks =
       tiles ? (tiles + ctx->opts.chunk_tiles - 1) / ctx->opts.chunk_tiles : 0;
-  const bool use_graph = ctx->opts.use_graphs != 0;
+  // Overlapped form: the chain walk of chunk c runs on a second stream while
+  // the sieve of chunk c+1 fills the other ring.
+  const bool two_streams = overlap && !count_only && nchunks > 1;
+  const bool use_graph = ctx->opts.use_graphs != 0 && !two_streams;
   const long long key = ((long long)ctx->variant << 40) | ((long long)(count_only ? 1 : 0) << 32) |
                         (long long)njobs;
   if (use_graph && (ctx->chunk_graph == nullptr || ctx->graph_key != key)) {
@@ -501,10 +556,10 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    chunk_begin_kernel<<<1, 1, 0, cs>>>(ctx->d_st);
-    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), cs>>>(sa);
-    if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, cs>>>(ca);
-    chunk_end_kernel<<<1, 1, 0, cs>>>(ctx->d_st, ctx->cand_cap);
+    chunk_begin_kernel<<<1, 1, 0, cs>>>(ctx->d_st, 0);
+    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), cs>>>(sa[0]);
+    if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, cs>>>(ca[0]);
+    chunk_end_kernel<<<1, 1, 0, cs>>>(ctx->d_st, ctx->cand_cap, 0);
     cudaError_t ce = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
@@ -522,18 +577,33 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     }
   }
   for (unsigned long long c = 0; c < nchunks; c++) {
+    const int r = two_streams ? (int)(c & 1) : 0;
     if (use_graph && !prof) {
       CK(cudaGraphLaunch(ctx->chunk_graph, s));
     } else {
-      chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st);
+      // ring r is free once the chain walk of chunk c-2 has read it
+      if (two_streams && c >= 2) CK(cudaStreamWaitEvent(s, ctx->chain_done[r], 0));
+      chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st, r);
       if (prof) CK(cudaEventRecord(ctx->prof_events[2 * c], s));
-      V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+      V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa[r]);
       if (prof) CK(cudaEventRecord(ctx->prof_events[2 * c + 1], s));
-      if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, s>>>(ca);
-      chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap);
+      if (two_streams) {
+        chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap, r);
+        CK(cudaEventRecord(ctx->sieve_done[r], s));
+        CK(cudaStreamWaitEvent(ctx->stream2, ctx->sieve_done[r], 0));
+        chain_kernel<<<ctx->chain_blocks, 128, 0, ctx->stream2>>>(ca[r]);
+        CK(cudaEventRecord(ctx->chain_done[r], ctx->stream2));
+      } else {
+        if (!count_only) chain_kernel<<<ctx->chain_blocks, 128, 0, s>>>(ca[r]);
+        chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap, r);
+      }
       CK(cudaGetLastError());
     }
     launches += count_only ? 3 : 4;
+  }
+  if (two_streams) {   // the last chain walks must finish before the read-back
+    CK(cudaStreamWaitEvent(s, ctx->chain_done[0], 0));
+    CK(cudaStreamWaitEvent(s, ctx->chain_done[1], 0));
   }
   CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(ctx->h_job_counts, ctx->d_job_counts, sizeof(unsigned long long) * njobs,
@@ -600,17 +670,17 @@ static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1
 
 // Runs jobs, retrying with smaller chunks on a candidate-buffer overflow.
 static int run_jobs_retry(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
-                          long long *n_aps) {
+                          long long *n_aps, bool overlap = false) {
   const int saved = ctx->opts.chunk_tiles;
   std::vector<KJob> keep(ctx->h_jobs, ctx->h_jobs + njobs);
-  int rc = run_jobs(ctx, njobs, count_only, stats, n_aps);
+  int rc = run_jobs(ctx, njobs, count_only, stats, n_aps, overlap);
   int tries = 0;
   while (rc == AP26_E_OVERFLOW && (ctx->h_st->err_flags & ERR_CAND_OVERFLOW) &&
          ctx->opts.chunk_tiles > 64 && tries < 6) {
     ctx->opts.chunk_tiles /= 4;
     if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
     memcpy(ctx->h_jobs, keep.data(), sizeof(KJob) * njobs);
-    rc = run_jobs(ctx, njobs, count_only, stats, n_aps);
+    rc = run_jobs(ctx, njobs, count_only, stats, n_aps, overlap);
     if (stats) stats->error_flags |= 1;
     tries++;
   }
@@ -666,7 +736,7 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
              N53_PER_K);
   long long n = 0;
   if (!jobs.empty()) {
-    rc = run_jobs_retry(ctx, (int)jobs.size(), false, stats, &n);
+    rc = run_jobs_retry(ctx, (int)jobs.size(), false, stats, &n, true);
     if (rc != AP26_OK) return rc;
   } else if (stats) {
     memset(stats, 0, sizeof(*stats));
@@ -736,7 +806,10 @@ extern "C" int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item) {
 extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
   if (!ctx) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  const int slice_k = std::max(1, ctx->num_sms / 8);
+  // One K-job per admitted unit per slice (round-robin), at most 8: a slice
+  // then lasts about one K of device time however many units are waiting,
+  // and a unit that arrives during a slice starts with the next one.
+  const int slice_k = std::max(1, std::min<int>(8, (int)ctx->units.size()));
   std::vector<std::pair<ServeUnit *, int>> picked;
   bool progress = true;
   while ((int)picked.size() < slice_k && progress) {
@@ -757,7 +830,7 @@ extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
                N53_PER_K);
     long long n = 0;
     ap26_stats st;
-    rc = run_jobs_retry(ctx, (int)picked.size(), false, &st, &n);
+    rc = run_jobs_retry(ctx, (int)picked.size(), false, &st, &n, true);
     if (rc != AP26_OK) {
       for (auto &pk : picked) pk.first->status = rc;
     } else {
@@ -841,22 +914,23 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
     CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->d_job_counts, 0, sizeof(unsigned long long), s));
     setup_jobs_kernel<<<1, 256, 0, s>>>(ctx->d_jobs, 1, ctx->d_tables);
-    chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st);
-    SieveArgs sa{ctx->d_jobs, 1, ctx->d_tables, ctx->d_st, ctx->d_cand, ctx->cand_cap,
-                 ctx->d_job_counts, 0};
+    chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st, 0);
+    const SieveArgs sa = sieve_args(ctx->d_jobs, 1, ctx->d_tables, ctx->d_st, ctx->d_cand[0],
+                                    ctx->cand_cap, ctx->d_job_counts, 0,
+                                    &ctx->d_st->cand_count[0]);
     V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(ctx->ev1, s));
     rc = wait_stream(ctx, 3600.0);
     if (rc == AP26_OK) {
-      const long long nc = (long long)ctx->h_st->cand_count;
+      const long long nc = (long long)ctx->h_st->cand_count[0];
       *n_cand = nc;
       if (nc > ctx->cand_cap) rc = AP26_E_OVERFLOW;
       else if (nc > cap) rc = AP26_E_CAPACITY;
       else if (nc > 0) {
         std::vector<Cand> tmp(nc);
-        CK(cudaMemcpy(tmp.data(), ctx->d_cand, sizeof(Cand) * nc, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tmp.data(), ctx->d_cand[0], sizeof(Cand) * nc, cudaMemcpyDeviceToHost));
         for (long long i = 0; i < nc; i++) cand[i] = tmp[i].n;
       }
       if (stats) {
@@ -1137,8 +1211,9 @@ extern "C" int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK,
     NoallocScratch *S = d->ptr;
     noalloc_init_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, d_Ks, nK, shift, V.WARPS * 32);
     setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0]);
-    chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st);
-    SieveArgs sa{S->jobs, nK, &S->tables[0][0], &S->st, nullptr, 0, S->counts, 1};
+    chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st, 0);
+    const SieveArgs sa = sieve_args(S->jobs, nK, &S->tables[0][0], &S->st, nullptr, 0,
+                                    S->counts, 1, &S->st.cand_count[0]);
     V.kernel<<<d->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
     noalloc_finish_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, nK, d_counts);
     if (cudaGetLastError() != cudaSuccess) rc = AP26_E_CUDA;

@@ -41,9 +41,8 @@ constexpr int PRIMES[NPRIMES] = {
     487, 491, 499, 503, 509, 521, 523, 541};
 
 // Each prime's bitstring covers p + WIN_EXTRA bits: enough for a 640-bit
-// window (plus a 32-bit funnel word) starting anywhere in [0, p).  The word
-// count is rounded up to even so every prime's segment starts 8-byte
-// aligned (the sieve reads the strings as 64-bit pairs).
+// window (plus a 32-bit funnel word) starting anywhere in [0, p), rounded
+// up to an even word count.
 constexpr int WIN_EXTRA = 672;
 constexpr int nwords(int p) { return ((p + WIN_EXTRA + 31) / 32 + 1) & ~1; }
 constexpr int word_offset(int g) {

@@ -69,7 +69,7 @@ struct APRec {
 struct DevState {
   unsigned long long tile_next, tile_end;      // current chunk window
   unsigned long long chunk_begin, chunk_size, total_tiles;
-  unsigned long long cand_count;               // per chunk
+  unsigned long long cand_count[2];            // per chunk, per candidate ring
   unsigned long long ap_count, prp_tests, cand_total, late_items;  // per run
   unsigned int err_flags;
   unsigned int pad;
@@ -90,6 +90,7 @@ struct SieveArgs {
   long long cand_cap;
   unsigned long long *job_counts;  // per-job survivor counts
   int count_only;               // 1: count survivors, emit no candidates
+  unsigned long long *cand_count;  // fill count of `cand` (DevState::cand_count[ring])
 };
 
 struct ChainArgs {
@@ -99,6 +100,7 @@ struct ChainArgs {
   long long cand_cap;
   APRec *aps;
   long long ap_cap;
+  const unsigned long long *cand_count;
 };
 
 // A tile is one n53 start per thread of a sieve CTA: WARPS * 32 starts.
@@ -130,12 +132,13 @@ __device__ __forceinline__ uint32_t window_start(uint32_t a, uint32_t b, uint32_
   return x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
 }
 
-// The shared table holds every bitstring twice: copy 0 at tab[0..), copy 1
-// (shifted down one word: copy1[i] = copy0[i+1]) at tab[TABLE_WORDS..).
-// Word w of a string is then the first half of an aligned 64-bit pair in
-// copy (w & 1), at index w & ~1.
+// The shared table holds the bitstrings as overlapping 64-bit pairs:
+// pair[i] = (word i, word i+1) for every i, so a window starting at any word
+// is a run of aligned 64-bit loads, pair[w], pair[w+2], ...; for a warp the
+// pairs read at one step lie within (p-1)/32 + 1 consecutive entries
+// (distinct banks or broadcast).
 __device__ __forceinline__ const uint2 *pair_at(const uint32_t *tab, uint32_t off, uint32_t w) {
-  return reinterpret_cast<const uint2 *>(tab + (w & 1u) * TABLE_WORDS + off + (w & ~1u));
+  return reinterpret_cast<const uint2 *>(tab) + off + w;
 }
 
 // All 640 bits (20 words) of prime g ANDed into acc: 11 pair loads, 20
@@ -150,7 +153,7 @@ __device__ __forceinline__ void dense_prime(const uint32_t *__restrict__ tab, ui
   uint32_t v[22];
 #pragma unroll
   for (int i = 0; i < 11; i++) {
-    const uint2 u = t[i];
+    const uint2 u = t[2 * i];
     v[2 * i] = u.x;
     v[2 * i + 1] = u.y;
   }
@@ -171,7 +174,7 @@ __device__ __forceinline__ void dense_pair(const uint32_t *__restrict__ tab, uin
   uint32_t vp[22], vq[22];
 #pragma unroll
   for (int i = 0; i < 11; i++) {
-    const uint2 u = tp[i], v = tq[i];
+    const uint2 u = tp[2 * i], v = tq[2 * i];
     vp[2 * i] = u.x;
     vp[2 * i + 1] = u.y;
     vq[2 * i] = v.x;
@@ -217,7 +220,7 @@ __device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w
     if (n % 7 && n % 11 && n % 13 && n % 17 && n % 19 && n % 23) {
       kept++;
       if (!A.count_only) {
-        unsigned long long i = atomicAdd(&A.st->cand_count, 1ull);
+        unsigned long long i = atomicAdd(A.cand_count, 1ull);
         if ((long long)i < A.cand_cap) {
           A.cand[i].n = n;
           A.cand[i].job = job;
@@ -239,7 +242,7 @@ __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
   const uint32_t pos = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k) + w64;
   const uint32_t w = pos >> 5;
   const uint2 u = *pair_at(tab, (uint32_t)P.off, w);
-  const uint32_t v2 = tab[P.off + w + 2];
+  const uint32_t v2 = pair_at(tab, (uint32_t)P.off, w + 2)->x;
   const uint32_t sh = pos & 31;
   lo &= __funnelshift_r(u.x, u.y, sh);
   hi &= __funnelshift_r(u.y, v2, sh);
@@ -426,8 +429,8 @@ sieve_kernel(SieveArgs A) {
       if (job < 0) break;
       const uint32_t *src = A.tables + (size_t)job * TABLE_WORDS;
       for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) {
-        tab[i] = src[i];
-        tab[TABLE_WORDS + i] = (i + 1 < TABLE_WORDS) ? src[i + 1] : 0u;
+        tab[2 * i] = src[i];
+        tab[2 * i + 1] = (i + 1 < TABLE_WORDS) ? src[i + 1] : 0u;
       }
       cur_job = job;
       cur_shift = A.jobs[job].shift;
@@ -552,7 +555,7 @@ __device__ __forceinline__ bool prp_term(DevState *st, int64_t m, unsigned &test
 
 // ---- chain walk: checkn.cl:128-206 / cpuavx2.cpp:532-552 ------------------------
 __global__ void chain_kernel(ChainArgs A) {
-  const unsigned long long n_c = min(A.st->cand_count, (unsigned long long)A.cand_cap);
+  const unsigned long long n_c = min(*A.cand_count, (unsigned long long)A.cand_cap);
   unsigned tests = 0, sq = 0;
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_c;
        i += (unsigned long long)gridDim.x * blockDim.x) {

@@ -206,6 +206,168 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---- extra workloads (not the default line) ----------------------------------------
+IMAD_PER_MULMOD = 12   # 32-bit multiply-adds of one 64-bit Montgomery product:
+                       # 4 for a*b, 3 for m = lo*n', 4 for hi(m*N), 1 carry
+
+
+def _base_line(metric, value, unit, args, world, workload, extra_cfg):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded)", "config": dict({"workload": workload}, **extra_cfg)}
+
+
+def workload_sieve(ctx, A, args, world, smem_gbs):
+    """Sieve only: survivor counts of consecutive K at SHIFT=640 (the sieve
+    roofline pair, 1024 K in the full configuration; --k-count sets the size)."""
+    import numpy as np
+    rng = np.random.default_rng(31)
+    k0 = int(rng.integers(1_000_000, 50_000_000 - args.k_count))
+    ks = [k for k in range(k0, k0 + args.k_count)]
+    ctx.sieve_count(ks[:2], 640)     # warm-up
+    counts, st = ctx.sieve_count(ks, 640)
+    cells = st.sieve_cells
+    achieved = cells * CONSULTS_PER_WORD * BYTES_PER_CONSULT / (st.sieve_ms / 1e3) / 1e9
+    line = _base_line("K/s, sieve only (10 shift words)", len(ks) / (st.device_ms / 1e3), "K/s",
+                      args, world, f"sieve survivor counts of {len(ks)} consecutive K from "
+                      f"{k0}, SHIFT=640", {"kmin": k0, "k_count": len(ks), "shift": 640})
+    line["roofline"] = {"bound": "smem", "achieved": achieved, "peak": smem_gbs, "unit": "GB/s",
+                        "frac": achieved / smem_gbs, "kernel": "sieve_kernel"}
+    line["survivors_total"] = int(counts.sum())
+    line["survivors_first"] = [int(c) for c in counts[:4]]
+    return line
+
+
+def workload_prp(ctx, A, args, world, int_tops):
+    """Strong-PRP microbenchmark: 2^prp_log2 odd values in [2^40, 2^63), half
+    primes (selected with the device test, a sample re-checked by the
+    oracle), half odd composites."""
+    import ctypes
+    import numpy as np
+    rng = np.random.default_rng(32)
+    n = 1 << args.prp_log2
+    want = n // 2
+    primes, comps = [], []
+    have_p = have_c = 0
+    while have_p < want or have_c < want:
+        cand = rng.integers(1 << 40, (1 << 63) - 1, 1 << 24, dtype=np.uint64) | np.uint64(1)
+        v, _ = ctx.sprp_batch(cand)
+        p, c = cand[v == 1], cand[v == 0]
+        primes.append(p[:max(0, want - have_p)])
+        comps.append(c[:max(0, want - have_c)])
+        have_p += len(primes[-1])
+        have_c += len(comps[-1])
+    vals = np.concatenate(primes + comps)
+    rng.shuffle(vals)
+    ctx.sprp_batch(vals[:1 << 16])
+    v, st = ctx.sprp_batch(vals)
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    idx = rng.integers(0, n, 4096)
+    ok = all(L.ao_sprp(ctypes.c_int64(int(vals[i])), ctypes.c_int64(2)) == int(v[i]) for i in idx)
+    squarings = st.late_items
+    mm_s = squarings / (st.device_ms / 1e3)
+    peak = int_tops * 1e12 / IMAD_PER_MULMOD
+    line = _base_line("base-2 SPRP tests/s", n / (st.device_ms / 1e3), "tests/s", args, world,
+                      f"{n} odd values in [2^40, 2^63), half primes", {"values": n})
+    line["mulmod_per_s"] = mm_s
+    line["roofline"] = {"bound": "int", "achieved": mm_s, "peak": peak, "unit": "mulmod/s",
+                        "frac": mm_s / peak, "kernel": "sprp_batch_kernel",
+                        "note": f"peak = measured IMAD rate / {IMAD_PER_MULMOD} multiply-adds "
+                                "per 64-bit Montgomery product; unit = modular squaring"}
+    line["primes"] = int(v.sum())
+    line["parity"] = {"oracle_sample": len(idx), "ok": bool(ok)}
+    return line
+
+
+def _mixed_items(rng, n, max_len, shifts=(0, 640, 1280)):
+    import math
+    items = []
+    for i in range(n):
+        length = int(math.exp(rng.uniform(0, math.log(max_len)))) if max_len > 1 else 1
+        length = max(1, min(max_len, length))
+        k0 = int(rng.integers(1_000_000, 50_000_000 - max_len))
+        items.append((i, k0, k0 + length - 1, int(rng.choice(shifts))))
+    return items
+
+
+def workload_batched(ctx, A, args, world):
+    """Batched persistent form vs plain one-K-per-launch-sequence form on the
+    same seeded mixed work items (log-uniform lengths 1..64 K, SHIFT from
+    {0, 640, 1280}); --items sets the count (4096 in the full configuration)."""
+    import numpy as np
+    rng = np.random.default_rng(44)
+    items = _mixed_items(rng, args.items, 64)
+    per, res, st = ctx.search_batch(items)
+    bms = st.device_ms
+    nk = sum(r.ks_searched for r in res)
+    t0 = time.perf_counter()
+    pms = 0.0
+    plain = []
+    for (iid, a, b, sh) in items:
+        reps = []
+        for K in range(a, b + 1):
+            if will_search(K):
+                r, s = ctx.search_k(K, sh)
+                pms += s.device_ms
+                reps += r
+        plain.append(reps)
+    same = all(p == q for p, q in zip(per, plain))
+    line = _base_line("K/s, batched persistent form", nk / (bms / 1e3), "K/s", args, world,
+                      f"{len(items)} items, log-uniform 1..64 K, SHIFT in {{0,640,1280}}",
+                      {"items": len(items), "searched_k": nk})
+    line["plain"] = {"value": nk / (pms / 1e3), "unit": "K/s"}
+    line["batched_over_plain"] = (nk / (bms / 1e3)) / (nk / (pms / 1e3))
+    line["parity"] = {"batched_equals_plain_per_item": same}
+    return line
+
+
+def workload_serve(ctx, A, args, world):
+    """Continuous-batching service: Poisson arrivals of units (log-uniform
+    1..--serve-max-k K, mixed SHIFT) at 80% of the measured batched
+    capacity; p50/p99 completion latency and sustained K/s."""
+    import numpy as np
+    rng = np.random.default_rng(55)
+    units = _mixed_items(rng, args.items, args.serve_max_k)
+    # capacity from one warm batch of 4 K
+    _, _, st = ctx.search_batch([(0, 2_000_003, 2_000_006, 0)])
+    cap_kps = 4 / (st.device_ms / 1e3)
+    mean_k = np.mean([sum(will_search(K) for K in range(a, b + 1)) for _, a, b, _ in units])
+    rate = 0.8 * cap_kps / max(mean_k, 1e-9)          # units per second
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(units)))
+    t0 = time.perf_counter()
+    nxt, done, lat, total_k = 0, 0, {}, 0
+    while done < len(units):
+        now = time.perf_counter() - t0
+        while nxt < len(units) and arrivals[nxt] <= now:
+            if ctx.serve_submit(*units[nxt]) != 0:
+                break
+            nxt += 1
+        active = ctx.serve_step()
+        while True:
+            r = ctx.serve_poll()
+            if r is None:
+                break
+            res, _aps = r
+            lat[res.id] = (time.perf_counter() - t0) - arrivals[res.id]
+            total_k += res.ks_searched
+            done += 1
+        if active == 0 and nxt < len(units):
+            time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+    span = time.perf_counter() - t0
+    ls = sorted(lat.values())
+    line = _base_line("serve p99 completion latency", float(np.percentile(ls, 99)), "s", args,
+                      world, f"{len(units)} Poisson units, log-uniform 1..{args.serve_max_k} K, "
+                      f"mixed SHIFT, arrivals at 0.8x capacity",
+                      {"units": len(units), "arrival_rate_units_per_s": rate,
+                       "capacity_kps": cap_kps})
+    line["higher_is_better"] = False
+    line["p50_s"] = float(np.percentile(ls, 50))
+    line["p99_s"] = float(np.percentile(ls, 99))
+    line["sustained_kps"] = total_k / span
+    return line
+
+
 # ---- our arm ---------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -216,6 +378,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--workload", default="range",
+                    choices=["range", "sieve", "prp", "batched", "serve"])
+    ap.add_argument("--k-count", type=int, default=64)
+    ap.add_argument("--prp-log2", type=int, default=24)
+    ap.add_argument("--items", type=int, default=16)
+    ap.add_argument("--serve-max-k", type=int, default=32)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -239,6 +407,21 @@ def main():
         tuned = ctx.autotune(KMIN_SEEDED + 64 * rank if will_search(KMIN_SEEDED + 64 * rank)
                              else KMIN_SEEDED)
     smem_gbs, int_tops = ctx.probe_peaks()
+    if args.workload != "range":
+        fn = {"sieve": lambda: workload_sieve(ctx, A, args, world, smem_gbs),
+              "prp": lambda: workload_prp(ctx, A, args, world, int_tops),
+              "batched": lambda: workload_batched(ctx, A, args, world),
+              "serve": lambda: workload_serve(ctx, A, args, world)}[args.workload]
+        with ClockSampler(local) as clk:
+            line = fn()
+        line["clocks"] = clk.summary()
+        line["autotuned"] = tuned
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     kmin, _ = replicas.rank_range(KMIN_SEEDED, RANGE_K, rank)
     nsteps_range = RANGE_K // STEP_K
 
