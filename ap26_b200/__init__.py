@@ -70,7 +70,7 @@ class ItemResult(ctypes.Structure):
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m ap26_b200.build` "
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python ap26_b200/build.py` "
                           "(there is no CPU fallback)")
     lib = ctypes.CDLL(LIB_PATH)
     P, I, I64, V = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, None

@@ -1,6 +1,6 @@
 """Build libap26.so and the `ap26` command in-tree for sm_100a.
 
-    python -m ap26_b200.build          (or ap26_b200.build.build())
+    python ap26_b200/build.py   (run by path: importing the package needs the library)
 
 Outputs (git-ignored, shipped with the working tree):
     ap26_b200/libap26.so   C ABI declared in include/ap26.h
