@@ -64,8 +64,25 @@ class Item(ctypes.Structure):
 class ItemResult(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int32), ("n_aps", ctypes.c_int32),
                 ("first_ap", ctypes.c_int64), ("candidates", ctypes.c_int64),
-                ("ks_searched", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("ks_searched", ctypes.c_int32), ("result_hash", ctypes.c_int32),
                 ("latency_ms", ctypes.c_double)]
+
+
+FINAL_MAX_SOL = 3
+
+
+class Final(ctypes.Structure):
+    """ap26_final: device-side ReportSolution of one raw report."""
+    _fields_ = [("hash_add", ctypes.c_int64), ("status", ctypes.c_int32),
+                ("n_sol", ctypes.c_int32), ("sol_len", ctypes.c_int32 * FINAL_MAX_SOL),
+                ("reserved", ctypes.c_int32), ("sol_first", ctypes.c_int64 * FINAL_MAX_SOL)]
+
+    def sols(self):
+        return [(self.sol_len[i], self.sol_first[i]) for i in range(self.n_sol)]
+
+
+class Sol(ctypes.Structure):
+    _fields_ = [("len", ctypes.c_int32), ("K", ctypes.c_int32), ("first", ctypes.c_int64)]
 
 
 def _load():
@@ -84,6 +101,9 @@ def _load():
         "ap26_set_opts": (I, [P, P]),
         "ap26_list_variants": (I, [P, I]),
         "ap26_search_k": (I, [P, I, I, P, I, P, P]),
+        "ap26_search_k_sol": (I, [P, I, I, P, P, I, P, P]),
+        "ap26_sprp_bases": (I, [P, P, P, I64, P, P]),
+        "ap26_report_batch": (I, [P, P, I64, P, P, P]),
         "ap26_search_batch": (I, [P, P, I, P, I64, P, P, P]),
         "ap26_serve_submit": (I, [P, P]),
         "ap26_serve_step": (I, [P, P]),
@@ -114,9 +134,11 @@ lib = _load()
 
 # Every symbol include/ap26.h declares (checked by the CPU test suite).
 EXPORTS = ("ap26_version", "ap26_strerror", "ap26_last_error", "ap26_create", "ap26_destroy",
-           "ap26_get_opts", "ap26_set_opts", "ap26_list_variants", "ap26_search_k", "ap26_search_batch", "ap26_serve_submit",
+           "ap26_get_opts", "ap26_set_opts", "ap26_list_variants", "ap26_search_k",
+           "ap26_search_k_sol", "ap26_search_batch", "ap26_serve_submit",
            "ap26_serve_step", "ap26_serve_poll", "ap26_sieve_range", "ap26_sieve_count",
-           "ap26_sprp_batch", "ap26_chain_batch", "ap26_autotune", "ap26_probe_peaks",
+           "ap26_sprp_batch", "ap26_sprp_bases", "ap26_report_batch", "ap26_chain_batch",
+           "ap26_autotune", "ap26_probe_peaks",
            "ap26_sieve_count_noalloc",
            "ap26_will_search",
            "ap26_report", "ap26_hash_hex", "ap26_sort_aps", "ap26_write_state",
@@ -250,6 +272,41 @@ class Context:
         self._check(lib.ap26_search_k(self.h, int(K), int(shift), out, cap, ctypes.byref(n),
                                       ctypes.byref(st)), "ap26_search_k")
         return _aps_to_list(out, n.value), st
+
+    def search_k_sol(self, K, shift=0, result_hash=0, cap=1 << 12):
+        """SearchAP26 + ReportSolution of every result on the device:
+        (new result_hash, SOL lines [(len, K, first)] in SOL order, stats)."""
+        out = (Sol * cap)()
+        h = ctypes.c_int32(result_hash)
+        n = ctypes.c_int(0)
+        st = Stats()
+        self._check(lib.ap26_search_k_sol(self.h, int(K), int(shift), ctypes.byref(h), out, cap,
+                                          ctypes.byref(n), ctypes.byref(st)),
+                    "ap26_search_k_sol")
+        return h.value, [(out[i].len, out[i].K, out[i].first) for i in range(n.value)], st
+
+    def report_batch(self, aps, result_hash=None):
+        """Device-side ReportSolution of raw reports [(k, K, first[, n])]:
+        returns (rc, [Final], new result_hash or None).  rc is the first
+        non-OK status (the per-report statuses are in the Finals)."""
+        arr = (AP * max(1, len(aps)))(*[AP(int(a[0]), int(a[1]), int(a[2]),
+                                           int(a[3]) if len(a) > 3 else 0) for a in aps])
+        fin = (Final * max(1, len(aps)))()
+        h = ctypes.c_int32(result_hash or 0)
+        rc = lib.ap26_report_batch(self.h, arr, len(aps), fin,
+                                   ctypes.byref(h) if result_hash is not None else None, None)
+        if rc in (E_CUDA, E_NODEV):
+            raise AP26Error(rc, "ap26_report_batch")
+        return rc, list(fin[:len(aps)]), (h.value if result_hash is not None else None)
+
+    def sprp_bases(self, N, a):
+        N = np.ascontiguousarray(N, dtype=np.uint64)
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        v = np.zeros(len(N), np.uint8)
+        st = Stats()
+        self._check(lib.ap26_sprp_bases(self.h, _ptr(N), _ptr(a), len(N), _ptr(v),
+                                        ctypes.byref(st)), "ap26_sprp_bases")
+        return v, st
 
     def search_batch(self, items, ap_cap=1 << 20):
         """items: [(id, kmin, kmax, shift)] -> (per-item list of reports, results, stats)."""

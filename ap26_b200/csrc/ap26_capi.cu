@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -139,6 +140,20 @@ __global__ void sprp_batch_kernel(const uint64_t *N, long long count, uint8_t *v
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(squarings, (unsigned long long)v);
 }
 
+// strong_prp(a, N) for explicit (N, a) pairs, a in [2, 31].
+__global__ void sprp_bases_kernel(const uint64_t *N, const uint32_t *a, long long count,
+                                  uint8_t *verdict) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    const uint64_t n = N[i];
+    const uint32_t b = a[i];
+    unsigned sq = 0;
+    bool v = false;
+    if ((n & 1) && n > b && n < (1ull << 63)) v = b == 2 ? sprp2(n, sq) : sprp_base(b, n);
+    verdict[i] = (uint8_t)v;
+  }
+}
+
 // Chain walk for explicit candidates (kernel-level parity entry point).
 __global__ void chain_explicit_kernel(const KJob *job, const int64_t *n, long long count,
                                       int32_t *k_out, int64_t *first_out, DevState *st) {
@@ -229,6 +244,7 @@ struct ServeUnit {
   int done_k = 0;
   std::vector<ap26_ap> aps;
   int64_t candidates = 0;
+  unsigned long long hash_add = 0;   // device-side ReportSolution hash sum
   int status = AP26_OK;
   std::chrono::steady_clock::time_point t_submit;
   double latency_ms = 0;
@@ -253,11 +269,14 @@ struct ap26_ctx {
   long long cand_cap = 0;
   APRec *d_aps = nullptr;
   long long ap_cap = 0;
+  FinRec *d_fin = nullptr;                   // ReportSolution result per report
+  unsigned long long *d_job_hash = nullptr;  // per-job sum of hash contributions
   // pinned host mirrors
   KJob *h_jobs = nullptr;
   DevState *h_st = nullptr;
   APRec *h_aps = nullptr;
-  unsigned long long *h_job_counts = nullptr;
+  FinRec *h_fin = nullptr;
+  unsigned long long *h_job_counts = nullptr, *h_job_hash = nullptr;
   // graphs
   cudaGraphExec_t chunk_graph = nullptr;
   long long graph_key = -1;
@@ -347,13 +366,16 @@ static int ensure_jobs(ap26_ctx *ctx, int njobs) {
   if (cap > 64 && need > ctx->opts.mem_budget) return AP26_E_NOMEM;
   if (ctx->d_jobs) {
     cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
-    cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts);
+    cudaFree(ctx->d_job_hash);
+    cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts); cudaFreeHost(ctx->h_job_hash);
   }
   CK(cudaMalloc(&ctx->d_jobs, sizeof(KJob) * cap));
   CK(cudaMalloc(&ctx->d_tables, sizeof(uint32_t) * TABLE_WORDS * (size_t)cap));
   CK(cudaMalloc(&ctx->d_job_counts, sizeof(unsigned long long) * cap));
+  CK(cudaMalloc(&ctx->d_job_hash, sizeof(unsigned long long) * cap));
   CK(cudaMallocHost(&ctx->h_jobs, sizeof(KJob) * cap));
   CK(cudaMallocHost(&ctx->h_job_counts, sizeof(unsigned long long) * cap));
+  CK(cudaMallocHost(&ctx->h_job_hash, sizeof(unsigned long long) * cap));
   ctx->jobs_cap = cap;
   if (ctx->chunk_graph) {
     cudaGraphExecDestroy(ctx->chunk_graph);
@@ -407,6 +429,8 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
       CKC(cudaEventCreateWithFlags(&ctx->chain_done[r], cudaEventDisableTiming));
     }
     CKC(cudaMalloc(&ctx->d_aps, sizeof(APRec) * ctx->ap_cap));
+    CKC(cudaMalloc(&ctx->d_fin, sizeof(FinRec) * ctx->ap_cap));
+    CKC(cudaMallocHost(&ctx->h_fin, sizeof(FinRec) * ctx->ap_cap));
     CKC(cudaMallocHost(&ctx->h_st, sizeof(DevState)));
     CKC(cudaMallocHost(&ctx->h_aps, sizeof(APRec) * ctx->ap_cap));
     if ((rc = ensure_jobs(ctx, 64)) != AP26_OK) goto fail;
@@ -429,6 +453,8 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
   for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
   cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
+  cudaFree(ctx->d_job_hash); cudaFree(ctx->d_fin);
+  cudaFreeHost(ctx->h_job_hash); cudaFreeHost(ctx->h_fin);
   cudaFree(ctx->d_st); cudaFree(ctx->d_cand[0]); cudaFree(ctx->d_cand[1]); cudaFree(ctx->d_aps);
   for (int r = 0; r < 2; r++) {
     if (ctx->sieve_done[r]) cudaEventDestroy(ctx->sieve_done[r]);
@@ -529,6 +555,7 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
   CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob) * njobs, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(ctx->d_job_counts, 0, sizeof(unsigned long long) * njobs, s));
+  CK(cudaMemsetAsync(ctx->d_job_hash, 0, sizeof(unsigned long long) * njobs, s));
   setup_jobs_kernel<<<njobs, 256, 0, s>>>(ctx->d_jobs, njobs, ctx->d_tables);
   CK(cudaGetLastError());
   int launches = 1;
@@ -605,14 +632,33 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     CK(cudaStreamWaitEvent(s, ctx->chain_done[0], 0));
     CK(cudaStreamWaitEvent(s, ctx->chain_done[1], 0));
   }
+  if (!count_only) {
+    // ReportSolution of every report on the device (AP26.cpp:549-602)
+    ReportArgs ra;
+    ra.aps = ctx->d_aps;
+    ra.count = &ctx->d_st->ap_count;
+    ra.n = ctx->ap_cap;
+    ra.jobs = ctx->d_jobs;
+    ra.fin = ctx->d_fin;
+    ra.job_hash = ctx->d_job_hash;
+    report_kernel<<<ctx->num_sms * 2, REPORT_WARPS * 32, 0, s>>>(ra);
+    CK(cudaGetLastError());
+    launches++;
+  }
   CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(ctx->h_job_counts, ctx->d_job_counts, sizeof(unsigned long long) * njobs,
                      cudaMemcpyDeviceToHost, s));
+  if (!count_only)
+    CK(cudaMemcpyAsync(ctx->h_job_hash, ctx->d_job_hash, sizeof(unsigned long long) * njobs,
+                       cudaMemcpyDeviceToHost, s));
   CK(cudaEventRecord(ctx->ev1, s));
   if ((rc = wait_stream(ctx, 3600.0)) != AP26_OK) return rc;
   long long n_aps = (long long)std::min<unsigned long long>(ctx->h_st->ap_count, ctx->ap_cap);
   if (n_aps > 0) {
     CK(cudaMemcpyAsync(ctx->h_aps, ctx->d_aps, sizeof(APRec) * n_aps, cudaMemcpyDeviceToHost, s));
+    if (!count_only)
+      CK(cudaMemcpyAsync(ctx->h_fin, ctx->d_fin, sizeof(FinRec) * n_aps, cudaMemcpyDeviceToHost,
+                         s));
     CK(cudaStreamSynchronize(s));
   }
   float ms = 0;
@@ -698,6 +744,55 @@ static void aprec_to_ap(const ap26_ctx *ctx, const APRec &r, ap26_ap &a) {
   a.n = r.n;
 }
 
+static_assert(sizeof(FinRec) == sizeof(ap26_final) && FIN_MAX_SOL == AP26_FINAL_MAX_SOL &&
+                  offsetof(FinRec, sol_first) == offsetof(ap26_final, sol_first),
+              "FinRec mirrors ap26_final");
+static_assert(sizeof(APRec) == sizeof(ap26_ap) && offsetof(APRec, first) == offsetof(ap26_ap, first),
+              "APRec mirrors ap26_ap (job in place of K)");
+static_assert(REP_INVALID == AP26_E_INVALID && REP_DOMAIN == AP26_E_DOMAIN &&
+                  REP_ARG == AP26_E_ARG && REP_OVERFLOW == AP26_E_OVERFLOW,
+              "report status codes are the public ones");
+
+constexpr long long kMaxIntV = 2000000000;   // MAXINTV, AP26.cpp:88
+
+// result_hash after adding `add` through ReportSolution calls, each of which
+// adds first%1000 + len and subtracts MAXINTV when above it (AP26.cpp:556-560):
+// for a start in [0, MAXINTV] the value stays in [0, MAXINTV], is congruent
+// to the total and is 0 only for a zero total.
+static int32_t hash_fold(int32_t h0, unsigned long long add) {
+  const unsigned long long total = (unsigned long long)h0 + add;
+  if (total == 0) return 0;
+  return (int32_t)((total - 1) % (unsigned long long)kMaxIntV + 1);
+}
+
+// A report with its ReportSolution result and AVX2 order key.
+struct RepOut {
+  ap26_ap ap;
+  FinRec fin;
+  uint64_t key;
+};
+
+// Reports of run_jobs' last call, job index alongside.
+static std::vector<std::pair<int, RepOut>> collect_reports(const ap26_ctx *ctx, long long n) {
+  std::vector<std::pair<int, RepOut>> v((size_t)n);
+  for (long long i = 0; i < n; i++) {
+    const APRec &r = ctx->h_aps[i];
+    v[i].first = r.job;
+    aprec_to_ap(ctx, r, v[i].second.ap);
+    v[i].second.fin = ctx->h_fin[i];
+    v[i].second.key = ap26h_order_key(v[i].second.ap.K, ctx->h_jobs[r.job].shift, r.n);
+  }
+  return v;
+}
+
+// The order ap26_sort_aps gives within one K: order key, first, k.
+static bool rep_less(const RepOut &x, const RepOut &y) {
+  if (x.ap.K != y.ap.K) return x.ap.K < y.ap.K;
+  if (x.key != y.key) return x.key < y.key;
+  if (x.ap.first != y.ap.first) return x.ap.first < y.ap.first;
+  return x.ap.k < y.ap.k;
+}
+
 extern "C" int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int cap,
                              int *n_out, ap26_stats *stats) {
   if (!ctx || !n_out || (cap > 0 && !out)) return AP26_E_ARG;
@@ -712,6 +807,44 @@ extern "C" int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int 
   if (n > cap) return AP26_E_CAPACITY;
   for (long long i = 0; i < n; i++) aprec_to_ap(ctx, ctx->h_aps[i], out[i]);
   ap26_sort_aps(out, (int)n, shift);
+  return AP26_OK;
+}
+
+extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int32_t *result_hash,
+                                 ap26_sol *sol, int cap, int *n_sol, ap26_stats *stats) {
+  if (!ctx || !result_hash || !n_sol || cap < 0 || (cap > 0 && !sol)) return AP26_E_ARG;
+  if (*result_hash < 0 || *result_hash > kMaxIntV) return AP26_E_ARG;
+  if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
+  if (!ap26_will_search(K)) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K);
+  long long n = 0;
+  int rc = run_jobs_retry(ctx, 1, false, stats, &n);
+  if (rc != AP26_OK) return rc;
+  auto v = collect_reports(ctx, n);
+  std::sort(v.begin(), v.end(),
+            [](const std::pair<int, RepOut> &x, const std::pair<int, RepOut> &y) {
+              return rep_less(x.second, y.second);
+            });
+  int ns = 0;
+  for (const auto &r : v) {
+    if (r.second.fin.status != AP26_OK) {
+      ctx->last_error = "ReportSolution failed for a report of K=" + std::to_string(K);
+      return r.second.fin.status;
+    }
+    ns += r.second.fin.n_sol;
+  }
+  *n_sol = ns;
+  if (ns > cap) return AP26_E_CAPACITY;
+  int o = 0;
+  for (const auto &r : v)
+    for (int i = 0; i < r.second.fin.n_sol; i++) {
+      sol[o].len = r.second.fin.sol_len[i];
+      sol[o].K = K;
+      sol[o].first = r.second.fin.sol_first[i];
+      o++;
+    }
+  *result_hash = hash_fold(*result_hash, ctx->h_job_hash[0]);
   return AP26_OK;
 }
 
@@ -742,30 +875,23 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
     memset(stats, 0, sizeof(*stats));
   }
   // group reports: item, K ascending, AVX2 order inside K
-  std::vector<std::vector<ap26_ap>> per_item(n_items);
-  for (long long i = 0; i < n; i++) {
-    const APRec &r = ctx->h_aps[i];
-    ap26_ap a;
-    aprec_to_ap(ctx, r, a);
-    per_item[ctx->h_jobs[r.job].item].push_back(a);
-  }
+  std::vector<std::vector<RepOut>> per_item(n_items);
+  for (auto &r : collect_reports(ctx, n)) per_item[ctx->h_jobs[r.first].item].push_back(r.second);
   int64_t total = 0;
+  std::vector<unsigned long long> hash_add(n_items, 0);
+  for (size_t j = 0; j < jobs.size(); j++) hash_add[jobs[j].first] += ctx->h_job_hash[j];
   for (int i = 0; i < n_items; i++) {
     auto &v = per_item[i];
-    std::stable_sort(v.begin(), v.end(), [](const ap26_ap &x, const ap26_ap &y) { return x.K < y.K; });
-    size_t b = 0;
-    while (b < v.size()) {
-      size_t e = b;
-      while (e < v.size() && v[e].K == v[b].K) e++;
-      ap26_sort_aps(v.data() + b, (int)(e - b), items[i].shift);
-      b = e;
-    }
+    std::sort(v.begin(), v.end(), rep_less);
     res[i].id = items[i].id;
     res[i].status = AP26_OK;
+    for (const auto &r : v)
+      if (r.fin.status != AP26_OK) { res[i].status = r.fin.status; break; }
     res[i].n_aps = (int32_t)v.size();
     res[i].first_ap = total;
     res[i].candidates = 0;
     res[i].ks_searched = 0;
+    res[i].result_hash = hash_fold(0, hash_add[i]);
     res[i].latency_ms = 0;
     total += (int64_t)v.size();
   }
@@ -776,8 +902,7 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
   *n_aps = total;
   if (total > ap_cap) return AP26_E_CAPACITY;
   for (int i = 0; i < n_items; i++)
-    if (!per_item[i].empty())
-      memcpy(aps + res[i].first_ap, per_item[i].data(), sizeof(ap26_ap) * per_item[i].size());
+    for (size_t e = 0; e < per_item[i].size(); e++) aps[res[i].first_ap + e] = per_item[i][e].ap;
   return AP26_OK;
 }
 
@@ -834,17 +959,17 @@ extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
     if (rc != AP26_OK) {
       for (auto &pk : picked) pk.first->status = rc;
     } else {
-      std::vector<std::vector<ap26_ap>> per_job(picked.size());
-      for (long long i = 0; i < n; i++) {
-        ap26_ap a;
-        aprec_to_ap(ctx, ctx->h_aps[i], a);
-        per_job[ctx->h_aps[i].job].push_back(a);
-      }
+      std::vector<std::vector<RepOut>> per_job(picked.size());
+      for (auto &r : collect_reports(ctx, n)) per_job[r.first].push_back(r.second);
       for (size_t j = 0; j < picked.size(); j++) {
         ServeUnit *u = picked[j].first;
-        ap26_sort_aps(per_job[j].data(), (int)per_job[j].size(), u->item.shift);
-        u->aps.insert(u->aps.end(), per_job[j].begin(), per_job[j].end());
+        std::sort(per_job[j].begin(), per_job[j].end(), rep_less);
+        for (const auto &r : per_job[j]) {
+          u->aps.push_back(r.ap);
+          if (r.fin.status != AP26_OK && u->status == AP26_OK) u->status = r.fin.status;
+        }
         u->candidates += (int64_t)ctx->h_job_counts[j];
+        u->hash_add += ctx->h_job_hash[j];
         u->done_k++;
       }
     }
@@ -878,6 +1003,7 @@ extern "C" int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *ap
   res->first_ap = 0;
   res->candidates = u.candidates;
   res->ks_searched = (int32_t)u.ks.size();
+  res->result_hash = hash_fold(0, u.hash_add);
   res->latency_ms = u.latency_ms;
   ctx->finished.pop_front();
   return 1;
@@ -997,6 +1123,85 @@ extern "C" int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count, 
     stats->launches = 1;
   }
   cudaFree(dN); cudaFree(dV); cudaFree(dsq);
+  return AP26_OK;
+}
+
+extern "C" int ap26_sprp_bases(ap26_ctx *ctx, const uint64_t *N, const uint32_t *a,
+                               int64_t count, uint8_t *verdict, ap26_stats *stats) {
+  if (!ctx || count < 0 || (count > 0 && (!N || !a || !verdict))) return AP26_E_ARG;
+  for (int64_t i = 0; i < count; i++)
+    if (a[i] < 2 || a[i] > 31) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (count == 0) return AP26_OK;
+  uint64_t *dN = nullptr;
+  uint32_t *dA = nullptr;
+  uint8_t *dV = nullptr;
+  CK(cudaMalloc(&dN, sizeof(uint64_t) * count));
+  CK(cudaMalloc(&dA, sizeof(uint32_t) * count));
+  CK(cudaMalloc(&dV, count));
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(dN, N, sizeof(uint64_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dA, a, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev0, s));
+  sprp_bases_kernel<<<ctx->num_sms * 16, 256, 0, s>>>(dN, dA, count, dV);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev1, s));
+  CK(cudaMemcpyAsync(verdict, dV, count, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->prp_tests = count;
+    stats->device_ms = ms;
+    stats->launches = 1;
+  }
+  cudaFree(dN); cudaFree(dA); cudaFree(dV);
+  return AP26_OK;
+}
+
+extern "C" int ap26_report_batch(ap26_ctx *ctx, const ap26_ap *raw, int64_t n, ap26_final *out,
+                                 int32_t *result_hash, ap26_stats *stats) {
+  if (!ctx || n < 0 || (n > 0 && (!raw || !out))) return AP26_E_ARG;
+  if (result_hash && (*result_hash < 0 || *result_hash > kMaxIntV)) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (n == 0) return AP26_OK;
+  APRec *dR = nullptr;
+  FinRec *dF = nullptr;
+  CK(cudaMalloc(&dR, sizeof(APRec) * n));
+  CK(cudaMalloc(&dF, sizeof(FinRec) * n));
+  cudaStream_t s = ctx->stream;
+  // ap26_ap and APRec share a layout; with jobs == null the job field is K
+  CK(cudaMemcpyAsync(dR, raw, sizeof(APRec) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev0, s));
+  ReportArgs ra;
+  ra.aps = dR;
+  ra.count = nullptr;
+  ra.n = n;
+  ra.jobs = nullptr;
+  ra.fin = dF;
+  ra.job_hash = nullptr;
+  const long long want = (n + REPORT_WARPS - 1) / REPORT_WARPS;
+  report_kernel<<<(int)std::min<long long>(want, ctx->num_sms * 8), REPORT_WARPS * 32, 0, s>>>(ra);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev1, s));
+  CK(cudaMemcpyAsync(out, dF, sizeof(FinRec) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (stats) {
+    stats->aps = n;
+    stats->device_ms = ms;
+    stats->launches = 1;
+  }
+  cudaFree(dR); cudaFree(dF);
+  unsigned long long add = 0;
+  for (int64_t i = 0; i < n; i++) {
+    if (out[i].status != AP26_OK) return out[i].status;
+    add += (unsigned long long)out[i].hash_add;
+  }
+  if (result_hash) *result_hash = hash_fold(*result_hash, add);
   return AP26_OK;
 }
 

@@ -6,9 +6,11 @@
  * every K in [KMIN, KMAX] with will_search(K), checkpoint before each K,
  * append "len K first" lines for APs of length >= 20 and, at the end, the
  * 16-hex-digit result hash to SOL-AP26.txt.  The per-K search runs on the
- * GPU through libap26.so (ap26_search_k in place of SearchAP26 at
- * AP26.cpp:976).  -batch N searches N K at a time through the batched
- * persistent form; output is identical.
+ * GPU through libap26.so: ap26_search_k_sol in place of SearchAP26 at
+ * AP26.cpp:976 and of the ReportSolution calls on its results (hash,
+ * 9-base validation and splits computed on the device).  -batch N searches
+ * N K at a time through the batched persistent form and reports through
+ * ap26_report_batch; output is identical.
  */
 #include <stdint.h>
 #include <stdio.h>
@@ -41,31 +43,37 @@ static void die(const char *msg) {
   exit(EXIT_FAILURE);
 }
 
-/* ReportSolution (AP26.cpp:549-602) through the library's hash/validation,
- * writing the SOL lines it produces. */
-static void report_all(const ap26_ap *aps, int n) {
+static void computation_error(void) {                      /* AP26.cpp:569-574 */
+  printf("Error: Computation error, found invalid AP, exiting...\n");
+  die("Error: Computation error, found invalid AP");
+}
+
+/* Appends solutions to SOL-AP26.txt (AP26.cpp:585-598). */
+static void write_sols(const ap26_sol *sol, int n) {
   for (int i = 0; i < n; i++) {
-    char sol[4096];
-    int sol_len = 0;
-    sol[0] = 0;
-    int rc = ap26_report(&result_hash, aps[i].k, aps[i].K, aps[i].first, sol, sizeof sol, &sol_len);
-    if (rc == AP26_E_INVALID) {
-      printf("Error: Computation error, found invalid AP, exiting...\n");
-      die("Error: Computation error, found invalid AP");
-    }
-    if (rc != AP26_OK) die(ap26_strerror(rc));
-    if (sol_len) {
-      if (!results_file) results_file = fopen(RESULTS_FILENAME, "a");
-      if (!results_file) die("Cannot open " RESULTS_FILENAME " !!!");
-      char *line = sol;
-      while (*line) {
-        char *nl = strchr(line, '\n');
-        printf("Solution: %.*s\n", (int)(nl - line), line);
-        line = nl + 1;
-      }
-      if (fputs(sol, results_file) < 0) die("Cannot write to " RESULTS_FILENAME " !!!");
-    }
+    if (!results_file) results_file = fopen(RESULTS_FILENAME, "a");
+    if (!results_file) die("Cannot open " RESULTS_FILENAME " !!!");
+    printf("Solution: %d %d %lld\n", sol[i].len, sol[i].K, (long long)sol[i].first);
+    if (fprintf(results_file, "%d %d %lld\n", sol[i].len, sol[i].K, (long long)sol[i].first) < 0)
+      die("Cannot write to " RESULTS_FILENAME " !!!");
   }
+}
+
+/* ReportSolution of raw reports, on the device (ap26_report_batch): the
+ * hash advances and the solutions are written in report order. */
+static void report_all(ap26_ctx *ctx, const ap26_ap *aps, int64_t n) {
+  if (n <= 0) return;
+  ap26_final *fin = (ap26_final *)malloc(sizeof(ap26_final) * (size_t)n);
+  if (!fin) die("out of memory");
+  int rc = ap26_report_batch(ctx, aps, n, fin, &result_hash, NULL);
+  if (rc == AP26_E_INVALID) computation_error();
+  if (rc != AP26_OK) die(ap26_strerror(rc));
+  for (int64_t i = 0; i < n; i++)
+    for (int j = 0; j < fin[i].n_sol; j++) {
+      ap26_sol s = {fin[i].sol_len[j], aps[i].K, fin[i].sol_first[j]};
+      write_sols(&s, 1);
+    }
+  free(fin);
 }
 
 static void write_hash_line(void) {                         /* AP26.cpp:295-357 */
@@ -133,6 +141,8 @@ int main(int argc, char **argv) {
 
   const int cap = 1 << 16;
   ap26_ap *aps = (ap26_ap *)malloc(sizeof(ap26_ap) * cap);
+  ap26_sol *sols = (ap26_sol *)malloc(sizeof(ap26_sol) * cap);
+  if (!aps || !sols) die("out of memory");
   while (K <= KMAX) {
     if (batch > 1) {
       /* next group of up to `batch` searchable K */
@@ -147,7 +157,7 @@ int main(int argc, char **argv) {
       time_t t0 = time(NULL);
       rc = ap26_search_batch(ctx, &it, 1, aps, cap, &n, &res, &st);
       if (rc != AP26_OK) die(ap26_strerror(rc));
-      report_all(aps, (int)n);
+      report_all(ctx, aps, n);
       fprintf(stderr, "K %d..%d done in %d sec (%.1f ms device).\n", K, kend - 1,
               (int)(time(NULL) - t0), st.device_ms);
       K_DONE += nk;
@@ -160,9 +170,11 @@ int main(int argc, char **argv) {
       int n = 0;
       ap26_stats st;
       time_t t0 = time(NULL);
-      rc = ap26_search_k(ctx, K, SHIFT, aps, cap, &n, &st);
+      /* SearchAP26 + ReportSolution of its results, both on the device */
+      rc = ap26_search_k_sol(ctx, K, SHIFT, &result_hash, sols, cap, &n, &st);
+      if (rc == AP26_E_INVALID) computation_error();
       if (rc != AP26_OK) die(ap26_strerror(rc));
-      report_all(aps, n);
+      write_sols(sols, n);
       fprintf(stderr, "K %d done in %d sec (%.1f ms device, %lld candidates).\n", K,
               (int)(time(NULL) - t0), st.device_ms, (long long)st.candidates);
       ITER = 0;
@@ -174,6 +186,7 @@ int main(int argc, char **argv) {
   write_hash_line();
   fprintf(stderr, "Workunit complete.\n");
   free(aps);
+  free(sols);
   ap26_destroy(ctx);
   return EXIT_SUCCESS;
 }

@@ -587,4 +587,182 @@ __global__ void chain_kernel(ChainArgs A) {
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(&A.st->prp_tests, (unsigned long long)v);
 }
 
+// ---- ReportSolution on the device: AP26.cpp:484-602 ------------------------------
+// Strong probable-prime test to base a (2 <= a < N), same verdict as the
+// reference's strong_prp(a, N) (PrimeQ_x86.h:143-182) for odd N in (a, 2^63):
+// x = a^d in Montgomery form, left to right, then up to t-1 squarings.
+__device__ __forceinline__ bool sprp_base(uint32_t a, uint64_t N) {
+  const uint64_t nm1 = N - 1;
+  const int t = __ffsll((long long)nm1) - 1;
+  const uint64_t d = nm1 >> t;
+  const uint64_t ninv = neg_inv64(N);
+  const uint64_t one = r_mod(N);
+  const uint64_t mone = N - one;
+  uint64_t am = 0;                      // a·2^64 mod N by double-and-add over a's bits
+  for (int b = 4; b >= 0; b--) {
+    am += am;
+    if (am >= N) am -= N;
+    if ((a >> b) & 1u) {
+      am += one;
+      if (am >= N) am -= N;
+    }
+  }
+  uint64_t x = am;
+  const int top = 63 - __clzll((long long)d);
+  for (int i = top - 1; i >= 0; i--) {
+    x = mont_mul(x, x, N, ninv);
+    if ((d >> i) & 1) x = mont_mul(x, am, N, ninv);
+  }
+  if (x == one || x == mone) return true;
+  for (int s = 1; s < t; s++) {
+    x = mont_mul(x, x, N, ninv);
+    if (x == mone) return true;
+    if (x == one) return false;
+  }
+  return false;
+}
+
+// Status codes of one report (the library's public codes).
+enum : int32_t { REP_OK = 0, REP_ARG = -1, REP_DOMAIN = -4, REP_OVERFLOW = -6, REP_INVALID = -8 };
+constexpr int FIN_MAX_SOL = 3;       // runs of >= 20 valid terms in one report of <= 128
+constexpr int FIN_MAX_TERMS = 128;
+constexpr int MIN_REPORT = 20;       // MINIMUM_AP_LENGTH_TO_REPORT, AP26.cpp:104
+
+// One raw report after ReportSolution (layout of the public ap26_final).
+struct FinRec {
+  int64_t hash_add;                  // sum of first%1000 + len over every call
+  int32_t status;
+  int32_t n_sol;
+  int32_t sol_len[FIN_MAX_SOL];
+  int32_t pad;
+  int64_t sol_first[FIN_MAX_SOL];
+};
+
+struct ReportArgs {
+  const APRec *aps;                  // k, job (or K when jobs is null), first
+  const unsigned long long *count;   // device-side report count, or null
+  long long n;                       // reports (cap when count is set)
+  const KJob *jobs;
+  FinRec *fin;
+  unsigned long long *job_hash;      // per-job sum of hash_add (status OK), or null
+};
+
+constexpr int REPORT_WARPS = 4;
+enum : uint8_t { TERM_DOM = 1, TERM_P2 = 2, TERM_P9 = 4 };
+
+// One warp per report: lane j tests terms j, j+32, ... (domain 0 <= N <
+// 2^62 of the reference's mulmod, AP26.cpp:494/529; base 2; the 8 further
+// bases of validate_ap26, AP26.cpp:519), then lane 0 replays the recursion
+// of ReportSolution over the per-term verdicts: every call adds
+// first%1000 + len; a piece whose first 9-base failure is at i is checked
+// to base 2 as a whole (Computation error otherwise), its leading i terms
+// are one call (valid, reported at length >= 20) and its trailing
+// len-(i+1) terms the next piece.
+__global__ void __launch_bounds__(REPORT_WARPS * 32) report_kernel(ReportArgs A) {
+  __shared__ uint8_t flags[REPORT_WARPS][FIN_MAX_TERMS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long n = A.count ? min((long long)*A.count, A.n) : A.n;
+  uint8_t *fl = flags[warp];
+  for (long long r = (long long)blockIdx.x * REPORT_WARPS + warp; r < n;
+       r += (long long)gridDim.x * REPORT_WARPS) {
+    const APRec rec = A.aps[r];
+    const int K = A.jobs ? A.jobs[rec.job].K : rec.job;
+    const int k = rec.k;
+    const int64_t first = rec.first;
+    FinRec out;
+    out.hash_add = 0;
+    out.status = REP_OK;
+    out.n_sol = 0;
+    out.pad = 0;
+    for (int i = 0; i < FIN_MAX_SOL; i++) { out.sol_len[i] = 0; out.sol_first[i] = 0; }
+    const bool args_ok = k >= 0 && first > 23 && K >= 1 && K <= 400000000;
+    if (args_ok && k > FIN_MAX_TERMS) out.status = REP_OVERFLOW;
+    else if (!args_ok) out.status = REP_ARG;
+    if (out.status == REP_OK) {
+      const uint64_t D = (uint64_t)K * (uint64_t)PRIM23;     // < 2^57
+      for (int j = lane; j < k; j += 32) {
+        uint8_t f = 0;
+        const uint64_t jd = (uint64_t)j * D;                   // < 2^64
+        const uint64_t N = (uint64_t)first + jd;
+        if (jd < (1ull << 62) && N < (1ull << 62)) {
+          f = TERM_DOM;
+          unsigned sq = 0;
+          if ((N & 1) && sprp2(N, sq)) {
+            f |= TERM_P2;
+            bool all = true;
+            const uint32_t bases[8] = {3, 5, 7, 11, 13, 17, 19, 23};
+            for (int b = 0; b < 8 && all; b++) all = sprp_base(bases[b], N);
+            if (all) f |= TERM_P9;
+          }
+        }
+        fl[j] = f;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      if (out.status == REP_OK) {
+        const int64_t D = (int64_t)K * PRIM23;
+        int s = 0;
+        const int e = k;
+        int64_t f = first;
+        for (;;) {
+          out.hash_add += f % 1000 + (e - s);
+          // validate_ap26 over [s, e): first term failing any of the 9 bases
+          int i = e;
+          if (f % 2 == 0) {
+            i = s;
+          } else {
+            for (int j = s; j < e; j++) {
+              if (!(fl[j] & TERM_DOM)) { out.status = REP_DOMAIN; break; }
+              if (!(fl[j] & TERM_P9)) { i = j; break; }
+            }
+          }
+          if (out.status != REP_OK) break;
+          if (i == e) {
+            if (e - s >= MIN_REPORT) {
+              if (out.n_sol < FIN_MAX_SOL) {
+                out.sol_len[out.n_sol] = e - s;
+                out.sol_first[out.n_sol] = f;
+                out.n_sol++;
+              } else {
+                out.status = REP_OVERFLOW;
+              }
+            }
+            break;
+          }
+          // Non-Solution: the whole piece must still be a base-2 AP
+          if (f % 2 == 0) {
+            out.status = REP_INVALID;
+            break;
+          }
+          for (int j = s; j < e; j++) {
+            if (!(fl[j] & TERM_DOM)) { out.status = REP_DOMAIN; break; }
+            if (!(fl[j] & TERM_P2)) { out.status = REP_INVALID; break; }
+          }
+          if (out.status != REP_OK) break;
+          // leading i-s terms: one call, valid by construction
+          out.hash_add += f % 1000 + (i - s);
+          if (i - s >= MIN_REPORT) {
+            if (out.n_sol < FIN_MAX_SOL) {
+              out.sol_len[out.n_sol] = i - s;
+              out.sol_first[out.n_sol] = f;
+              out.n_sol++;
+            } else {
+              out.status = REP_OVERFLOW;
+              break;
+            }
+          }
+          // trailing piece
+          f += (int64_t)(i + 1 - s) * D;
+          s = i + 1;
+        }
+      }
+      A.fin[r] = out;
+      if (A.job_hash && out.status == REP_OK)
+        atomicAdd(&A.job_hash[rec.job], (unsigned long long)out.hash_add);
+    }
+    __syncwarp();
+  }
+}
+
 }  // namespace ap26

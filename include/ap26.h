@@ -103,9 +103,38 @@ typedef struct {
   int64_t first_ap;     /* index of its first report in the caller's array   */
   int64_t candidates;   /* sieve survivors over all its K                    */
   int32_t ks_searched;  /* K with will_search(K) true                        */
-  int32_t reserved;
+  int32_t result_hash;  /* the reference's result_hash after ReportSolution
+                           of all the item's reports, starting from 0
+                           (AP26.cpp:556-560), computed on the device        */
   double latency_ms;    /* serving: admission-to-completion wall time        */
 } ap26_item_result;
+
+/* ReportSolution (src/common/AP26.cpp:549-602) of one raw report, computed
+ * on the device: the report's call and every call its split recursion makes
+ * add first%1000 + len to the hash; pieces that pass the 9-base validation
+ * (validate_ap26, AP26.cpp:513-543) with len >= 20 are solutions, in the
+ * order the reference appends them to SOL-AP26.txt. */
+#define AP26_FINAL_MAX_SOL 3
+typedef struct {
+  int64_t hash_add;     /* sum of first%1000 + len over all those calls      */
+  int32_t status;       /* AP26_OK; AP26_E_INVALID: a piece is not even a
+                           base-2 AP ("Computation error", AP26.cpp:569-574);
+                           AP26_E_DOMAIN: a term outside [0, 2^62)
+                           (AP26.cpp:529-533); AP26_E_ARG: k < 0, first <= 23
+                           or K outside [1, AP26_KMAX_SAFE]; AP26_E_OVERFLOW:
+                           k > 128 or more than AP26_FINAL_MAX_SOL solutions */
+  int32_t n_sol;        /* solutions (len >= 20) in sol_len / sol_first       */
+  int32_t sol_len[AP26_FINAL_MAX_SOL];
+  int32_t reserved;
+  int64_t sol_first[AP26_FINAL_MAX_SOL];
+} ap26_final;
+
+/* One line of SOL-AP26.txt: "len K first" (AP26.cpp:593). */
+typedef struct {
+  int32_t len;
+  int32_t K;
+  int64_t first;
+} ap26_sol;
 
 /* ---- library / context --------------------------------------------------- */
 int ap26_version(void);
@@ -136,6 +165,17 @@ int ap26_list_variants(ap26_opts *out, int cap);
  * own ReportSolution).  K must satisfy ap26_will_search(K). */
 int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int cap,
                   int *n_out, ap26_stats *stats);
+
+/* The whole per-K step of the reference's K loop (AP26.cpp:976, SearchAP26
+ * followed by ReportSolution of every result) with the reporting done on
+ * the device: *result_hash (in [0, 2e9]) is advanced exactly as the
+ * reference's ReportSolution calls advance result_hash, and the solutions
+ * (9-base valid, len >= 20) are written to sol[0..cap) in the order the
+ * reference appends them to SOL-AP26.txt; *n_sol = count.  Errors:
+ * AP26_E_INVALID / AP26_E_DOMAIN where the reference exits (then
+ * *result_hash is unchanged), AP26_E_CAPACITY (*n_sol holds the need). */
+int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int32_t *result_hash,
+                      ap26_sol *sol, int cap, int *n_sol, ap26_stats *stats);
 
 /* ---- batched persistent form ----------------------------------------------
  * All searchable K of all items in one persistent work-stealing pipeline:
@@ -174,6 +214,18 @@ int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int shift,
  * src/common/PrimeQ_x86.h:143-182). */
 int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count,
                     uint8_t *verdict, ap26_stats *stats);
+/* strong_prp(a[i], N[i]) verdicts (src/common/PrimeQ_x86.h:143-182) for
+ * the validation bases: a[i] in [2, 31] (AP26_E_ARG otherwise); verdict 0
+ * for even N, N <= a or N >= 2^63. */
+int ap26_sprp_bases(ap26_ctx *ctx, const uint64_t *N, const uint32_t *a, int64_t count,
+                    uint8_t *verdict, ap26_stats *stats);
+/* ReportSolution of n given raw reports on the device, one ap26_final each
+ * (the same values the reference's recursion produces).  If result_hash is
+ * not NULL and every report is AP26_OK, *result_hash (in [0, 2e9]) is
+ * advanced by all of them; otherwise the first non-OK status is returned
+ * and *result_hash is unchanged. */
+int ap26_report_batch(ap26_ctx *ctx, const ap26_ap *raw, int64_t n, ap26_final *out,
+                      int32_t *result_hash, ap26_stats *stats);
 /* Chain walk for given candidates n of K (checkn.cl:128-206): k and first
  * per candidate (first undefined when k < 10). */
 int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,

@@ -8,6 +8,9 @@
 #   oracle/_ref/ref_harness  oracle/ref_harness.cpp linked with the reference's
 #                            Search_avx2 / Search_sse2 objects (raw AP records and
 #                            bounded timing samples)
+#   oracle/_ref/ref_primeq   the reference's strong_prp on "N a" pairs
+#   oracle/_ref/ref_report   the reference's ReportSolution on one raw report
+#                            (AP26.cpp compiled again with main renamed)
 #
 # Flags follow the reference's own makefile (src/cpu/Makefile_linux:10-38) minus
 # BOINC: -O3 -m64, per-file -mavx2 / -mavx / -msse4.1 / -msse2.
@@ -35,3 +38,8 @@ $CXX -o "$OUT/ref_harness" "$OUT/ref_harness.o" "$OUT/cpuavx2.o" "$OUT/cpusse2.o
 echo "built $OUT/AP26 $OUT/ref_harness"
 $CXX $CF -o "$OUT/ref_primeq" "$HERE/ref_primeq.cpp"
 echo "built $OUT/ref_primeq"
+$CXX $CF -Dmain=ap26_reference_main -c -o "$OUT/AP26_nomain.o" "$REF/src/common/AP26.cpp"
+$CXX $CF -c -o "$OUT/ref_report.o" "$HERE/ref_report.cpp"
+$CXX -o "$OUT/ref_report" "$OUT/ref_report.o" "$OUT/AP26_nomain.o" "$OUT/cpuavx2.o" \
+     "$OUT/cpuavx.o" "$OUT/cpusse41.o" "$OUT/cpusse2.o" -lm
+echo "built $OUT/ref_report"

@@ -204,6 +204,9 @@ def test_batch_equals_plain(ctx):
                 exp += ctx.search_k(K, shift)[0]
         assert reps == exp
         assert r.n_aps == len(exp)
+        rep = A.Reporter()
+        rep.report_all(exp)
+        assert r.result_hash == rep.hash.value   # device-side ReportSolution
 
 
 def test_serving_alone_equals_mixed(ctx):
@@ -216,6 +219,9 @@ def test_serving_alone_equals_mixed(ctx):
         r = ctx.serve_poll()
         assert r is not None and r[0].id == u[0]
         alone[u[0]] = r[1]
+        rep = A.Reporter()
+        rep.report_all(r[1])
+        assert r[0].result_hash == rep.hash.value
     assert ctx.serve_poll() is None
     for u in units:
         assert ctx.serve_submit(*u) == 0
@@ -228,10 +234,14 @@ def test_serving_alone_equals_mixed(ctx):
         r = ctx.serve_poll()
         if r is None:
             break
-        mixed[r[0].id] = r[1]
+        mixed[r[0].id] = (r[0], r[1])
     for u in units:
-        assert mixed[u[0]] == alone[u[0]]
+        assert mixed[u[0]][1] == alone[u[0]]
     assert 4 in mixed
+    for uid, (res, aps) in mixed.items():
+        rep = A.Reporter()
+        rep.report_all(aps)
+        assert res.result_hash == rep.hash.value, uid
 
 
 def test_serving_admission_by_memory_budget():

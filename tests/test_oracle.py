@@ -29,6 +29,30 @@ def test_oracle_report_matches_golden(oracle, K):
     assert oracle_sol(oracle, K, ref_raw(K)) == golden_sol(K)
 
 
+def test_oracle_report_matches_reference_report_vectors(oracle):
+    """ao_report against the reference's own ReportSolution on single raw
+    reports (tests/golden/report_vectors.txt): splits around base-2
+    pseudoprimes, the 9-base-passing composite, exits and hash wrap-around."""
+    n_exit = 0
+    with open(os.path.join(GOLDEN, "report_vectors.txt")) as f:
+        for ln in f:
+            if ln.startswith("#"):
+                continue
+            k, K, first, h0, st, h, sols = ln.split()
+            hh = ctypes.c_int(int(h0))
+            buf = ctypes.create_string_buffer(1 << 12)
+            rc = oracle.ao_report(ctypes.byref(hh), int(k), int(K), ctypes.c_int64(int(first)),
+                                  buf, len(buf))
+            if st == "exit":
+                assert rc < 0, ln
+                n_exit += 1
+                continue
+            assert rc == 0 and hh.value == int(h), ln
+            got = [f"{x.split()[0]}:{x.split()[2]}" for x in buf.value.decode().splitlines()]
+            assert (",".join(got) or "-") == sols, ln
+    assert n_exit >= 4
+
+
 def sprp_vectors():
     out = []
     with open(os.path.join(GOLDEN, "sprp_vectors.txt")) as f:
