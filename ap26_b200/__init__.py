@@ -101,7 +101,7 @@ def _load():
         "ap26_set_opts": (I, [P, P]),
         "ap26_list_variants": (I, [P, I]),
         "ap26_search_k": (I, [P, I, I, P, I, P, P]),
-        "ap26_search_k_sol": (I, [P, I, I, P, P, I, P, P]),
+        "ap26_search_k_sol": (I, [P, I, I, I, P, P, I, P, P]),
         "ap26_sprp_bases": (I, [P, P, P, I64, P, P]),
         "ap26_report_batch": (I, [P, P, I64, P, P, P]),
         "ap26_search_batch": (I, [P, P, I, P, I64, P, P, P]),
@@ -273,15 +273,16 @@ class Context:
                                       ctypes.byref(st)), "ap26_search_k")
         return _aps_to_list(out, n.value), st
 
-    def search_k_sol(self, K, shift=0, result_hash=0, cap=1 << 12):
-        """SearchAP26 + ReportSolution of every result on the device:
-        (new result_hash, SOL lines [(len, K, first)] in SOL order, stats)."""
+    def search_k_sol(self, K, shift=0, result_hash=0, iter=0, cap=1 << 12):
+        """SearchAP26 + ReportSolution of every result on the device, from
+        shift word `iter` (the reference's ITER) on: (new result_hash, SOL
+        lines [(len, K, first)] in SOL order, stats)."""
         out = (Sol * cap)()
         h = ctypes.c_int32(result_hash)
         n = ctypes.c_int(0)
         st = Stats()
-        self._check(lib.ap26_search_k_sol(self.h, int(K), int(shift), ctypes.byref(h), out, cap,
-                                          ctypes.byref(n), ctypes.byref(st)),
+        self._check(lib.ap26_search_k_sol(self.h, int(K), int(shift), int(iter), ctypes.byref(h),
+                                          out, cap, ctypes.byref(n), ctypes.byref(st)),
                     "ap26_search_k_sol")
         return h.value, [(out[i].len, out[i].K, out[i].first) for i in range(n.value)], st
 

@@ -705,13 +705,15 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
   return AP26_OK;
 }
 
-static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1) {
+static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1,
+                     int word_begin = 0) {
   memset(&J, 0, sizeof(J));
   J.K = K;
   J.shift = shift;
   J.item = item;
   J.q_begin = q0;
   J.q_end = q1;
+  J.word_begin = word_begin;
 }
 
 // Runs jobs, retrying with smaller chunks on a candidate-buffer overflow.
@@ -810,14 +812,16 @@ extern "C" int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int 
   return AP26_OK;
 }
 
-extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int32_t *result_hash,
-                                 ap26_sol *sol, int cap, int *n_sol, ap26_stats *stats) {
+extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
+                                 int32_t *result_hash, ap26_sol *sol, int cap, int *n_sol,
+                                 ap26_stats *stats) {
   if (!ctx || !result_hash || !n_sol || cap < 0 || (cap > 0 && !sol)) return AP26_E_ARG;
+  if (iter < 0 || iter >= WORDS) return AP26_E_ARG;
   if (*result_hash < 0 || *result_hash > kMaxIntV) return AP26_E_ARG;
   if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
   if (!ap26_will_search(K)) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K);
+  fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K, iter);
   long long n = 0;
   int rc = run_jobs_retry(ctx, 1, false, stats, &n);
   if (rc != AP26_OK) return rc;

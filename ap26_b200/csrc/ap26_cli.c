@@ -108,13 +108,19 @@ int main(int argc, char **argv) {
                       &write_state_a_next)) {
     printf("Resuming search from checkpoint.\n");
     fprintf(stderr, "Resuming from checkpoint. K: %d ITER: %d\n", K, ITER);
-    if (ITER != 0) {   /* GPU builds restart a K from its first word (AP26.cpp:792-801) */
+    if (ITER < 0 || ITER > 9) {   /* not a shift word: restart (AP26.cpp:792-801) */
       printf("Checkpoint was from a different version. Restarting workunit.\n");
       fprintf(stderr, "Checkpoint was from a different version. Restarting workunit.\n");
       K = KMIN;
       ITER = 0;
       result_hash = 0;
       last_trickle = (double)time(NULL);
+    } else if (ITER != 0) {
+      /* A mid-K checkpoint of the reference's CPU build (ITER 4 or 8 before
+         its 4-word passes): the reference's GPU build restarts the workunit
+         here; this one continues K at shift word ITER with the hash of the
+         words before it, which gives the uninterrupted run's output. */
+      fprintf(stderr, "Continuing K %d from shift word %d.\n", K, ITER);
     }
   } else {
     printf("Beginning a new search with parameters from the command line\n");
@@ -144,7 +150,7 @@ int main(int argc, char **argv) {
   ap26_sol *sols = (ap26_sol *)malloc(sizeof(ap26_sol) * cap);
   if (!aps || !sols) die("out of memory");
   while (K <= KMAX) {
-    if (batch > 1) {
+    if (batch > 1 && ITER == 0) {   /* a K resumed mid-way goes through the per-K path */
       /* next group of up to `batch` searchable K */
       int kend = K, nk = 0;
       while (kend <= KMAX && nk < batch) { if (ap26_will_search(kend)) nk++; kend++; }
@@ -171,7 +177,7 @@ int main(int argc, char **argv) {
       ap26_stats st;
       time_t t0 = time(NULL);
       /* SearchAP26 + ReportSolution of its results, both on the device */
-      rc = ap26_search_k_sol(ctx, K, SHIFT, &result_hash, sols, cap, &n, &st);
+      rc = ap26_search_k_sol(ctx, K, SHIFT, ITER, &result_hash, sols, cap, &n, &st);
       if (rc == AP26_E_INVALID) computation_error();
       if (rc != AP26_OK) die(ap26_strerror(rc));
       write_sols(sols, n);

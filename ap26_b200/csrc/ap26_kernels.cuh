@@ -51,6 +51,8 @@ struct KJob {
   int64_t q_begin, q_end;     // n53 start range [q_begin, q_end)
   int64_t tile_begin;         // global index of this job's first tile
   int32_t K, shift, item, ntiles;
+  int32_t word_begin;         // first shift word reported (the reference's ITER)
+  int32_t pad;
 };
 
 struct Cand {
@@ -295,11 +297,14 @@ __device__ __forceinline__ int late_drain(const SieveArgs &A, const uint32_t *ta
                                           int &n, int lane, int shift, int job) {
   tail_stages<R>(tab, buf, n, lane, SL, NPRIMES);
   int kept = 0;
+  // a K resumed at shift word ITER reports words ITER..9 only
+  const int word_begin = A.jobs[job].word_begin;
   for (int i = lane; i < n; i += 32) {
     const uint4 it = buf[i];
     const uint64_t n59 = (uint64_t)it.x | ((uint64_t)(it.y & 0xffffu) << 32);
-    kept += emit_word(A, n59, (int)((it.y >> 16) & 15u), ((uint64_t)it.w << 32) | it.z, shift,
-                      job);
+    const int w = (int)((it.y >> 16) & 15u);
+    if (w >= word_begin)
+      kept += emit_word(A, n59, w, ((uint64_t)it.w << 32) | it.z, shift, job);
   }
   __syncwarp();
   n = 0;

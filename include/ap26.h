@@ -171,10 +171,15 @@ int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int cap,
  * the device: *result_hash (in [0, 2e9]) is advanced exactly as the
  * reference's ReportSolution calls advance result_hash, and the solutions
  * (9-base valid, len >= 20) are written to sol[0..cap) in the order the
- * reference appends them to SOL-AP26.txt; *n_sol = count.  Errors:
- * AP26_E_INVALID / AP26_E_DOMAIN where the reference exits (then
- * *result_hash is unchanged), AP26_E_CAPACITY (*n_sol holds the need). */
-int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int32_t *result_hash,
+ * reference appends them to SOL-AP26.txt; *n_sol = count.
+ * iter is the reference's ITER, the first of the 10 shift words to report:
+ * 0 for a whole K; a checkpoint of the reference's CPU build holds 4 or 8
+ * (written before its second and third 4-word pass, cpuavx2.cpp:860) with
+ * the hash of the words before it, and iter = that ITER continues the K
+ * exactly (any 0..9 is accepted).  Errors: AP26_E_INVALID / AP26_E_DOMAIN
+ * where the reference exits (then *result_hash is unchanged),
+ * AP26_E_CAPACITY (*n_sol holds the need). */
+int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter, int32_t *result_hash,
                       ap26_sol *sol, int cap, int *n_sol, ap26_stats *stats);
 
 /* ---- batched persistent form ----------------------------------------------

@@ -57,3 +57,30 @@ def test_cli_batched_form_writes_same_output(tmp_path):
     run_cli(a, 1000037, 1000041, 640)
     run_cli(b, 1000037, 1000041, 640, "-batch", 3)
     assert (a / "SOL-AP26.txt").read_text() == (b / "SOL-AP26.txt").read_text()
+
+
+def test_cli_continues_reference_mid_k_checkpoint(tmp_path):
+    """A state written by the reference CPU build before its second 4-word
+    pass (K=366384, ITER=4, hash 48373; tests/golden/ref_states.txt), with the
+    SOL lines it had written by then: the command continues the K at shift
+    word 4 and ends with the golden SOL file."""
+    mid = {}
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ref_states.txt")) as f:
+        for ln in f:
+            if not ln.startswith("#"):
+                kmin, kmax, shift, K, it, h = map(int, ln.split())
+                mid[(K, it)] = h
+    K = 366384
+    with A.Context(0) as c:
+        _, sols_all, _ = c.search_k_sol(K, 0)
+        _, sols_tail, _ = c.search_k_sol(K, 0, result_hash=mid[(K, 4)], iter=4)
+    head = sols_all[:len(sols_all) - len(sols_tail)]
+    (tmp_path / "AP26-state.a.txt").write_text(f"{K} {K} 0 {K} 4 {mid[(K, 4)]} 0.000000\n")
+    (tmp_path / "SOL-AP26.txt").write_text("".join(f"{a} {b} {c}\n" for a, b, c in head))
+    p = run_cli(tmp_path, K, K, 0)
+    assert "Continuing K 366384 from shift word 4" in p.stderr
+    assert (tmp_path / "SOL-AP26.txt").read_text() == golden_sol(K)
+    states = [(tmp_path / f).read_text().split()[:6]
+              for f in ("AP26-state.a.txt", "AP26-state.b.txt")]
+    assert [str(K), str(K), "0", str(K + 1), "0", "87376"] in states
+

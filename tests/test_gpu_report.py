@@ -176,3 +176,37 @@ def test_search_k_sol_continues_hash(ctx):
     h, sols, _ = ctx.search_k_sol(K, 0, result_hash=1999999500)
     assert h == r.hash.value
     assert [f"{a} {b} {c}" for a, b, c in sols] == r.sol
+
+
+def ref_states():
+    """Checkpoints the reference CPU build wrote while searching the golden K
+    (tests/golden/make_ref_states.py): {K: {ITER: result_hash}}, and the
+    final hash of each K (the state with K + 1, ITER 0)."""
+    mid, final = {}, {}
+    with open(os.path.join(GOLDEN, "ref_states.txt")) as f:
+        for ln in f:
+            if ln.startswith("#"):
+                continue
+            kmin, kmax, shift, K, it, h = map(int, ln.split())
+            if K == kmax + 1:
+                final[kmin] = h
+            elif it:
+                mid.setdefault(K, {})[it] = h
+    return mid, final
+
+
+@pytest.mark.parametrize("K", GOLDEN_KS)
+def test_search_k_sol_continues_reference_mid_k_checkpoints(ctx, K):
+    """From the reference's checkpoint at ITER 4 and 8 (hash of shift words
+    0..ITER-1), the rest of the K ends at the reference's final hash; its
+    solutions are the tail of the whole-K solutions."""
+    mid, final = ref_states()
+    assert sorted(mid[K]) == [4, 8]
+    h_all, sols_all, _ = ctx.search_k_sol(K, 0, result_hash=0)
+    assert h_all == final[K]
+    for it, h0 in mid[K].items():
+        h, sols, st = ctx.search_k_sol(K, 0, result_hash=h0, iter=it)
+        assert h == final[K], (K, it)
+        assert sols == sols_all[len(sols_all) - len(sols):], (K, it)
+    with pytest.raises(A.AP26Error):
+        ctx.search_k_sol(K, 0, iter=10)
