@@ -71,6 +71,9 @@ def oracle_sieve(oracle, K, shift, q0, q1, threads=4):
     (1000039, 1280, 12_345_678, 12_370_000),
     (49999981, 0, 77_777_777, 77_800_000),
     (43241056 + 5, 16000 - 640, 1000, 20000),  # largest SHIFT in the domain
+    (1, 0, 0, 30_000),                         # smallest K
+    (2, 1280, 9_000_000, 9_013_000),
+    (400_000_000, 640, 5_000_000, 5_020_000),  # largest K in the domain (AP26_KMAX_SAFE)
 ])
 def test_sieve_range_vs_oracle(ctx, oracle, K, shift, q0, q1):
     if not A.will_search(K):
@@ -116,9 +119,10 @@ def test_sieve_rejects_bad_ranges(ctx):
 
 
 # ---- chain walk ----------------------------------------------------------------
-def test_chain_vs_oracle(ctx, oracle):
-    K = 366384
-    cand, _ = ctx.sieve_range(K, 0, 0, 3 * 12673)
+@pytest.mark.parametrize("K,shift", [(366384, 0), (1, 0), (400_000_000, 640),
+                                     (43241061, 16000 - 640)])
+def test_chain_vs_oracle(ctx, oracle, K, shift):
+    cand, _ = ctx.sieve_range(K, shift, 0, 3 * 12673)
     k, first, st = ctx.chain_batch(K, cand)
     STEP = K * A.PRIM23
     kk = ctypes.c_int()
@@ -172,15 +176,27 @@ def test_search_k_matches_pinned_candidate_counts(ctx):
         assert counts[0] == p["candidates"]
 
 
+def recorded_reference_ks():
+    """(K, SHIFT) of every recorded reference raw-report file
+    (tests/golden/ref_raw/shift<SHIFT>/<K>.txt)."""
+    out = []
+    for d in sorted(glob.glob(os.path.join(GOLDEN, "ref_raw", "shift*"))):
+        shift = int(os.path.basename(d)[5:])
+        out += [(int(os.path.basename(f)[:-4]), shift)
+                for f in sorted(glob.glob(os.path.join(d, "*.txt")))]
+    return out
+
+
 def test_recorded_reference_ranges(ctx):
-    """Every K with a recorded reference raw-report file (tests/golden/
-    ref_raw/shift0): device reports equal the reference's, in order."""
-    files = sorted(glob.glob(os.path.join(GOLDEN, "ref_raw", "shift0", "*.txt")))
-    ks = [int(os.path.basename(f)[:-4]) for f in files]
-    assert len(ks) >= 3
-    for K in ks:
-        aps, st = ctx.search_k(K, 0)
-        assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(K), K
+    """Every K with a recorded reference raw-report file, at every recorded
+    SHIFT (0, and 640 / 1280 / 15360 for seeded K): device reports equal
+    the reference's, in order."""
+    cases = recorded_reference_ks()
+    assert len(cases) >= 3 and len({s for _, s in cases}) >= 1
+    for K, shift in cases:
+        aps, st = ctx.search_k(K, shift)
+        assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(K, shift), (K, shift)
+        assert st.error_flags == 0
 
 
 def test_search_k_rejects_unsearchable_and_out_of_domain(ctx):
