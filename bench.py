@@ -19,6 +19,8 @@ search).
            launch time, against the measured shared-memory peak
   cpu_baseline  the reference CPU build (oracle/_ref/ref_harness: the
            reference's own Search_avx2) on every host core, bounded samples
+  cpu_avx512    companion: the AVX-512 restatement of the same search
+           (oracle/ap26_avx512.c) on every host core, bounded sample
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -38,6 +40,7 @@ KMIN_SEEDED = 43241056          # numpy default_rng(26).integers(1_000_000, 50_0
 RANGE_K = 64
 STEP_K = 8
 SHIFT = 0
+N59_PER_K = 4808136200          # lattice positions per K (10840 n43 x 443555)
 CONSULTS_PER_WORD = 16.62       # oracle: mean table lookups per shift word (canonical order)
 BYTES_PER_CONSULT = 8
 # H2D/D2H payload per K-job and per call (sizes of the C ABI structures)
@@ -101,20 +104,37 @@ class ClockSampler:
 
 
 # ---- CPU baseline: the reference's own search on all host cores ------------------
+PASS_ITERS = (0, 4, 8)          # Search_avx2's three passes (shift words 0-3, 4-7, 8-9)
+N43_PER_PASS = 10840
+
+
 def ref_sample(ks, ticks):
-    """Runs ref_harness sample K 0 ticks for each K concurrently; returns
-    (K-equivalents searched, wall seconds, processes)."""
+    """One ref_harness process per host core, all concurrent: process i
+    runs the pass starting at shift word PASS_ITERS[i % 3] of K ks[i] and is
+    stopped after `ticks` of the pass's 85 (i31, i37) pairs.  Each pass's
+    time per lattice value comes from the first tick to the stop (its table
+    set-up is timed separately), so a K costs
+    sum over passes of (set-up + 10840 x time per value).
+    Returns (K/s on these cores, wall seconds, processes)."""
     t0 = time.time()
-    procs = [subprocess.Popen([REF_HARNESS, "sample", str(k), str(SHIFT), str(ticks)],
-                              stdout=subprocess.PIPE, text=True) for k in ks]
-    frac = 0.0
+    procs = [subprocess.Popen([REF_HARNESS, "sample", str(k), str(SHIFT), str(ticks), "avx2",
+                               str(PASS_ITERS[i % len(PASS_ITERS)])],
+                              stdout=subprocess.PIPE, text=True) for i, k in enumerate(ks)]
+    per_value = {it: [] for it in PASS_ITERS}
+    setup = {it: [] for it in PASS_ITERS}
     for p in procs:
         out, _ = p.communicate()
         for ln in out.splitlines():
             if ln.startswith("SAMPLE"):
-                _, _k, done, total, secs, _isa = ln.split()
-                frac += int(done) / int(total)
-    return frac, time.time() - t0, len(ks)
+                f = ln.split()
+                done, it, setup_s, tick_s = int(f[2]), int(f[6]), float(f[7]), float(f[8])
+                if done > 0:
+                    per_value[it].append(tick_s / done)
+                    setup[it].append(setup_s)
+    wall = time.time() - t0
+    k_seconds = sum(statistics.mean(setup[it]) + N43_PER_PASS * statistics.mean(per_value[it])
+                    for it in PASS_ITERS)
+    return len(ks) / k_seconds, wall, len(ks)
 
 
 def port_sample(ks, seconds=10.0):
@@ -142,16 +162,50 @@ def port_sample(ks, seconds=10.0):
 def cpu_baseline_value(ks_pool, ticks):
     ncores = os.cpu_count() or 1
     ks = [ks_pool[i % len(ks_pool)] for i in range(ncores)]
-    if os.access(REF_HARNESS, os.X_OK):
-        frac, secs, n = ref_sample(ks, ticks)
+    if os.access(REF_HARNESS, os.X_OK) and ncores >= len(PASS_ITERS):
+        kps, secs, n = ref_sample(ks, ticks)
         kind = "reference"
-        sample = (f"reference Search_avx2 (oracle/_ref/ref_harness), {n} processes x first "
-                  f"{ticks} progress ticks of pass 0 of one K each (SHIFT=0, K from the workload)")
+        sample = (f"reference Search_avx2 (oracle/_ref/ref_harness), {n} concurrent processes, "
+                  f"each the first {ticks} of 85 progress ticks of one of the 3 passes of one K "
+                  "(SHIFT=0, K from the workload); per-pass time per lattice value x 10840 + "
+                  "set-up, summed over the passes")
     else:
         frac, secs, n = port_sample(ks)
+        kps = frac / secs
         kind = "port"
         sample = f"oracle port, {n} threads x 2e6 lattice values of one K each"
-    return {"value": frac / secs, "unit": "K/s", "cores": n, "kind": kind, "sample": sample,
+    return {"value": kps, "unit": "K/s", "cores": n, "kind": kind, "sample": sample,
+            "seconds": round(secs, 2)}
+
+
+def avx512_companion(k, seconds=8.0):
+    """The AVX-512 restatement (oracle/ap26_avx512.c: sieve + chain walk) on
+    every host core over a bounded lattice slice of one K of the workload,
+    sized from a short calibration run to take about `seconds`; None on a
+    CPU without AVX-512 VBMI2."""
+    import ctypes
+    import numpy as np
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    if not L.a5_supported():
+        return None
+    L.a5_search.restype = ctypes.c_int64
+    ncores = os.cpu_count() or 1
+    cap = 1 << 16
+    bufs = [np.zeros(cap, t) for t in (np.int32, np.int64, np.int64, np.uint64)]
+    def run(span):
+        t0 = time.time()
+        n = L.a5_search(k, SHIFT, ctypes.c_int64(0), ctypes.c_int64(span),
+                        *[b.ctypes.data_as(ctypes.c_void_p) for b in bufs],
+                        ctypes.c_int64(cap), None, ncores)
+        assert n >= 0
+        return time.time() - t0
+    cal = 200_000 * ncores
+    t = run(cal)
+    span = int(min(N59_PER_K, max(cal, cal * seconds / max(t, 1e-3))))
+    secs = run(span)
+    return {"value": span / N59_PER_K / secs, "unit": "K/s", "cores": ncores, "kind": "port",
+            "sample": f"AVX-512 restatement (oracle/ap26_avx512.c), {ncores} threads over "
+                      f"lattice positions [0, {span}) of K={k} (SHIFT=0)",
             "seconds": round(secs, 2)}
 
 
@@ -554,6 +608,9 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             ks = [k for k in range(KMIN_SEEDED, KMIN_SEEDED + RANGE_K) if will_search(k)]
             line["cpu_baseline"] = cpu_baseline_value(ks, 6)
+            comp = avx512_companion(ks[0])
+            if comp:
+                line["cpu_avx512"] = comp
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -19,8 +19,14 @@
  *
  * Modes:
  *   ref_harness raw    K SHIFT [avx2|sse2]   -> "R k K first" lines + summary
- *   ref_harness sample K SHIFT TICKS [avx2|sse2]
- *                      -> "SAMPLE K n43_done total_n43_units seconds"
+ *   ref_harness sample K SHIFT TICKS [avx2|sse2] [ITER]
+ *                      -> "SAMPLE K n43_done total_n43_units seconds isa ITER
+ *                          setup_seconds tick_seconds"
+ *                      the pass starting at shift word ITER (0, 4 or 8 for
+ *                      AVX2: Search_avx2's own resume point), aborted after
+ *                      TICKS pairs; setup_seconds = start to the first tick
+ *                      (tables of the pass), tick_seconds = first tick to the
+ *                      abort (exactly n43_done lattice values of the pass)
  *
  * Progress accounting (sample mode): the AVX2 search calls Progress once per
  * admissible (i31, i37) pair of each 4-word pass (cpuavx2.cpp:380-388), the
@@ -44,13 +50,19 @@ void Search_sse2(int K, int startSHIFT, int ITER, int K_COUNT, int K_DONE);
 
 static int g_mode_sample = 0;
 static long g_ticks = 0, g_tick_limit = 0;
+static double g_t_first = 0, g_t_end = 0;
+static double now_s(void);
 static jmp_buf g_abort;
 static long g_reports = 0;
 
 void Progress(double prog) {
   (void)prog;
   g_ticks++;
-  if (g_mode_sample && g_ticks > g_tick_limit) longjmp(g_abort, 1);
+  if (g_ticks == 1) g_t_first = now_s();
+  if (g_mode_sample && g_ticks > g_tick_limit) {
+    g_t_end = now_s();
+    longjmp(g_abort, 1);
+  }
 }
 
 void ReportSolution(int AP_Length, int difference, int64_t First_Term) {
@@ -93,11 +105,13 @@ int main(int argc, char **argv) {
   int K = atoi(argv[2]);
   int SHIFT = atoi(argv[3]);
   const char *isa = "avx2";
+  int iter = 0;
   if (!strcmp(argv[1], "sample")) {
     if (argc < 5) return 2;
     g_mode_sample = 1;
     g_tick_limit = atol(argv[4]);
     if (argc > 5) isa = argv[5];
+    if (argc > 6) iter = atoi(argv[6]);
   } else if (argc > 4) {
     isa = argv[4];
   }
@@ -106,16 +120,18 @@ int main(int argc, char **argv) {
 
   double t0 = now_s();
   if (setjmp(g_abort) == 0) {
-    if (use_sse2) Search_sse2(K, SHIFT, 0, 1, 0);
-    else Search_avx2(K, SHIFT, 0, 1, 0);
+    if (use_sse2) Search_sse2(K, SHIFT, iter, 1, 0);
+    else Search_avx2(K, SHIFT, iter, 1, 0);
   }
   double dt = now_s() - t0;
   fflush(stdout);
   if (g_mode_sample) {
-    long T = g_ticks - 1;           /* pairs fully searched in pass 0 */
+    long T = g_ticks - 1;           /* pairs fully searched in the pass */
     if (T < 0) T = 0;
     long done = n43_in_first_pairs(T);
-    printf("SAMPLE %d %ld %ld %.6f %s\n", K, done, 10840L * passes, dt, isa);
+    if (g_t_end == 0) g_t_end = now_s();   /* the pass ended before the limit */
+    printf("SAMPLE %d %ld %ld %.6f %s %d %.6f %.6f\n", K, done, 10840L * passes, dt, isa, iter,
+           g_t_first - t0, g_t_end - g_t_first);
   } else {
     printf("DONE %d %ld %.3f %s\n", K, g_reports, dt, isa);
   }

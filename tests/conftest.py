@@ -21,8 +21,9 @@ def pytest_configure(config):
 
 def _oracle_lib():
     path = os.path.join(ROOT, "oracle", "liboracle.so")
-    src = os.path.join(ROOT, "oracle", "ap26_oracle.c")
-    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+    srcs = [os.path.join(ROOT, "oracle", f) for f in ("ap26_oracle.c", "ap26_avx512.c")]
+    if not os.path.exists(path) or any(os.path.getmtime(path) < os.path.getmtime(s)
+                                       for s in srcs):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"],
                        check=True)
     L = ctypes.CDLL(path)
@@ -31,6 +32,8 @@ def _oracle_lib():
     L.ao_n59.restype = ctypes.c_int64
     L.ao_avx2_order_key.restype = ctypes.c_uint64
     L.ao_avx2_order_key.argtypes = [ctypes.c_uint64]
+    L.a5_sieve.restype = ctypes.c_int64
+    L.a5_search.restype = ctypes.c_int64
     return L
 
 
