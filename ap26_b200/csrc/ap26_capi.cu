@@ -218,14 +218,15 @@ struct SieveVariant {
 
 // (dense primes, tail group, late stage, queue, late queue, warps per CTA)
 static const SieveVariant kVariants[] = {
-    AP26_VARIANT(20, 4, 44, 320, 96, 8),   // default
+    AP26_VARIANT(22, 6, 52, 320, 96, 8),   // default
+    AP26_VARIANT(22, 6, 52, 320, 96, 12),
+    AP26_VARIANT(24, 8, 56, 320, 96, 8),
+    AP26_VARIANT(20, 6, 44, 320, 96, 12),
+    AP26_VARIANT(20, 4, 44, 320, 96, 8),
     AP26_VARIANT(16, 4, 44, 320, 96, 8),
-    AP26_VARIANT(24, 4, 44, 320, 96, 8),
     AP26_VARIANT(24, 4, 52, 320, 96, 8),
     AP26_VARIANT(28, 4, 52, 320, 96, 8),
     AP26_VARIANT(20, 4, 44, 384, 128, 8),
-    AP26_VARIANT(24, 4, 52, 384, 128, 8),
-    AP26_VARIANT(20, 4, 44, 320, 96, 12),
     AP26_VARIANT(24, 4, 52, 320, 96, 12),
     AP26_VARIANT(20, 4, 44, 320, 96, 4),
 };
