@@ -35,8 +35,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("dense_primes", ctypes.c_int32), ("warp_queue", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("late_stage", ctypes.c_int32),
                 ("chunk_tiles", ctypes.c_int32), ("use_graphs", ctypes.c_int32),
-                ("profile", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("mem_budget", ctypes.c_int64)]
+                ("profile", ctypes.c_int32), ("cand_ring_log2", ctypes.c_int32),
+                ("mem_budget", ctypes.c_int64), ("wait_timeout_s", ctypes.c_double)]
 
 
 class AP(ctypes.Structure):

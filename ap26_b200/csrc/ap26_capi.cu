@@ -287,7 +287,18 @@ struct ap26_ctx {
   std::deque<ServeUnit> finished;
   int64_t bytes_in_use = 0;     // device bytes held by admitted serving units
   std::string last_error;
+  bool pending = false;        // a call timed out with its work still queued
 };
+
+// A call that gave up waiting (AP26_E_TIMEOUT) left its work queued, and its
+// read-backs still target the pinned host mirrors: the next call that reuses
+// them waits for that work first.
+static void drain(ap26_ctx *ctx) {
+  if (!ctx->pending) return;
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->stream2);
+  ctx->pending = false;
+}
 
 static int cuda_fail(ap26_ctx *ctx, cudaError_t e, const char *what) {
   if (ctx) ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
@@ -328,6 +339,8 @@ static int default_opts(ap26_opts *o) {
   if (!o->late_stage) o->late_stage = kVariants[0].SL;
   if (!o->chunk_tiles) o->chunk_tiles = 32768;
   if (!o->mem_budget) o->mem_budget = (int64_t)8 << 30;
+  if (!o->cand_ring_log2) o->cand_ring_log2 = 23;
+  if (!(o->wait_timeout_s > 0)) o->wait_timeout_s = 3600.0;
   return 0;
 }
 
@@ -419,7 +432,11 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     for (int g = 0; g < NPRIMES; g++) params[g] = make_param(g);
     CKC(cudaMemcpyToSymbol(c_params, params, sizeof(params)));
     // buffers
-    ctx->cand_cap = 8ll << 20;
+    if (ctx->opts.cand_ring_log2 < 12 || ctx->opts.cand_ring_log2 > 26) {
+      rc = AP26_E_ARG;
+      goto fail;
+    }
+    ctx->cand_cap = 1ll << ctx->opts.cand_ring_log2;
     ctx->ap_cap = 1ll << 20;
     CKC(cudaMalloc(&ctx->d_st, sizeof(DevState)));
     CKC(cudaMalloc(&ctx->d_cand[0], sizeof(Cand) * ctx->cand_cap));
@@ -451,6 +468,7 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
   if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
   for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
   cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
@@ -490,11 +508,22 @@ extern "C" int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts) {
   if (opts->late_stage) o.late_stage = opts->late_stage;
   if (opts->chunk_tiles) o.chunk_tiles = opts->chunk_tiles;
   if (opts->mem_budget) o.mem_budget = opts->mem_budget;
+  if (opts->cand_ring_log2) o.cand_ring_log2 = opts->cand_ring_log2;
+  if (opts->wait_timeout_s > 0) o.wait_timeout_s = opts->wait_timeout_s;
   o.use_graphs = opts->use_graphs;
   o.profile = opts->profile;
   const int vi = pick_variant(o);
-  if (vi < 0) return AP26_E_ARG;
+  if (vi < 0 || o.cand_ring_log2 < 12 || o.cand_ring_log2 > 26) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
+  if (o.cand_ring_log2 != ctx->opts.cand_ring_log2) {
+    cudaFree(ctx->d_cand[0]);
+    cudaFree(ctx->d_cand[1]);
+    ctx->d_cand[0] = ctx->d_cand[1] = nullptr;
+    ctx->cand_cap = 1ll << o.cand_ring_log2;
+    CK(cudaMalloc(&ctx->d_cand[0], sizeof(Cand) * ctx->cand_cap));
+    CK(cudaMalloc(&ctx->d_cand[1], sizeof(Cand) * ctx->cand_cap));
+  }
   const int64_t keep_budget = o.mem_budget;
   ctx->opts = o;
   int rc = set_variant(ctx, vi);
@@ -524,6 +553,7 @@ static int wait_stream(ap26_ctx *ctx, double timeout_s) {
     double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (el > timeout_s) {
       ctx->last_error = "device wait exceeded the timeout";
+      ctx->pending = true;
       return AP26_E_TIMEOUT;
     }
     std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 20 : 200));
@@ -536,6 +566,7 @@ static int wait_stream(ap26_ctx *ctx, double timeout_s) {
 static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
                     long long *n_aps_out, bool overlap = false) {
   int rc;
+  drain(ctx);
   if ((rc = ensure_jobs(ctx, njobs)) != AP26_OK) return rc;
   // tile prefix; a tile is one start per thread of the variant's CTA
   const SieveVariant &V = kVariants[ctx->variant];
@@ -653,7 +684,7 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     CK(cudaMemcpyAsync(ctx->h_job_hash, ctx->d_job_hash, sizeof(unsigned long long) * njobs,
                        cudaMemcpyDeviceToHost, s));
   CK(cudaEventRecord(ctx->ev1, s));
-  if ((rc = wait_stream(ctx, 3600.0)) != AP26_OK) return rc;
+  if ((rc = wait_stream(ctx, ctx->opts.wait_timeout_s)) != AP26_OK) return rc;
   long long n_aps = (long long)std::min<unsigned long long>(ctx->h_st->ap_count, ctx->ap_cap);
   if (n_aps > 0) {
     CK(cudaMemcpyAsync(ctx->h_aps, ctx->d_aps, sizeof(APRec) * n_aps, cudaMemcpyDeviceToHost, s));
@@ -802,6 +833,7 @@ extern "C" int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int 
   if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
   if (!ap26_will_search(K)) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K);
   long long n = 0;
   int rc = run_jobs_retry(ctx, 1, false, stats, &n);
@@ -822,6 +854,7 @@ extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
   if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
   if (!ap26_will_search(K)) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K, iter);
   long long n = 0;
   int rc = run_jobs_retry(ctx, 1, false, stats, &n);
@@ -859,6 +892,7 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
                                  ap26_item_result *res, ap26_stats *stats) {
   if (!ctx || !items || n_items < 0 || !n_aps || !res) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   std::vector<std::pair<int, int>> jobs;   // (item, K)
   for (int i = 0; i < n_items; i++) {
     const ap26_item &it = items[i];
@@ -936,6 +970,7 @@ extern "C" int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item) {
 extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
   if (!ctx) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   // One K-job per admitted unit per slice (round-robin), at most 8: a slice
   // then lasts about one K of device time however many units are waiting,
   // and a unit that arrives during a slice starts with the next one.
@@ -1020,6 +1055,7 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
   if (!ctx || !n_cand || q_begin < 0 || q_end > N53_PER_K || q_end < q_begin) return AP26_E_ARG;
   if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   fill_job(ctx->h_jobs[0], K, shift, 0, q_begin, q_end);
   // sieve without the chain walk: one chunk covering everything, candidates kept
   const int saved = ctx->opts.chunk_tiles;
@@ -1053,7 +1089,7 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(ctx->ev1, s));
-    rc = wait_stream(ctx, 3600.0);
+    rc = wait_stream(ctx, ctx->opts.wait_timeout_s);
     if (rc == AP26_OK) {
       const long long nc = (long long)ctx->h_st->cand_count[0];
       *n_cand = nc;
@@ -1085,6 +1121,7 @@ extern "C" int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int sh
                                 int64_t *counts, ap26_stats *stats) {
   if (!ctx || !Ks || nK <= 0 || !counts) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   int rc;
   if ((rc = ensure_jobs(ctx, nK)) != AP26_OK) return rc;
   for (int i = 0; i < nK; i++) {
@@ -1215,6 +1252,7 @@ extern "C" int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t 
   if (!ctx || (count > 0 && (!n || !k_out || !first_out)) || count < 0) return AP26_E_ARG;
   if (!k_in_domain(K, 0)) return AP26_E_DOMAIN;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   if (count == 0) return AP26_OK;
   fill_job(ctx->h_jobs[0], K, 0, 0, 0, 0);
   int64_t *dn = nullptr, *df = nullptr;
@@ -1286,6 +1324,7 @@ extern "C" int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen)
   if (!ctx) return AP26_E_ARG;
   if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
   CK(cudaSetDevice(ctx->device));
+  drain(ctx);
   const int64_t q1 = N53_PER_K / 64;
   double best_ms = 1e30;
   int best_v = ctx->variant, best_chunk = ctx->opts.chunk_tiles;

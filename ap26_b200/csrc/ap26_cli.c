@@ -1,5 +1,5 @@
 /* ap26_cli.c -- the `ap26` command: AP26 KMIN KMAX SHIFT [-compute]
- *                [-device N] [-batch N]
+ *                [-device N] [-batch N] [-stop-after N]
  *
  * Keeps the reference's command-line contract (ibethune/ap26
  * src/common/AP26.cpp:660-1041): resume from AP26-state.{a,b}.txt, search
@@ -10,7 +10,10 @@
  * AP26.cpp:976 and of the ReportSolution calls on its results (hash,
  * 9-base validation and splits computed on the device).  -batch N searches
  * N K at a time through the batched persistent form and reports through
- * ap26_report_batch; output is identical.
+ * ap26_report_batch; output is identical.  -stop-after N ends the process
+ * after N searched K with the checkpoint of the next K written and no hash
+ * line, the way a BOINC client stops a task between K; running the command
+ * again resumes there.
  */
 #include <stdint.h>
 #include <stdio.h>
@@ -87,13 +90,14 @@ static void write_hash_line(void) {                         /* AP26.cpp:295-357 
 }
 
 int main(int argc, char **argv) {
-  int K, SHIFT, ITER = 0, device = 0, batch = 0;
+  int K, SHIFT, ITER = 0, device = 0, batch = 0, stop_after = 0, searched = 0;
   printf("AP26 B200 10-shift search version 1.0 (sm_100a, libap26 %d)\n", ap26_version());
   fprintf(stderr, "Command line: ");
   for (int i = 0; i < argc; i++) fprintf(stderr, "%s ", argv[i]);
   fprintf(stderr, "\n");
   if (argc < 4) {
-    printf("Usage: %s KMIN KMAX SHIFT [-compute] [-device N] [-batch N]\n", argv[0]);
+    printf("Usage: %s KMIN KMAX SHIFT [-compute] [-device N] [-batch N] [-stop-after N]\n",
+           argv[0]);
     exit(EXIT_FAILURE);
   }
   sscanf(argv[1], "%d", &KMIN);
@@ -103,6 +107,7 @@ int main(int argc, char **argv) {
     if (!strcmp(argv[i], "-compute")) fprintf(stderr, "Compute mode enabled.\n");
     else if (!strcmp(argv[i], "-device") && i + 1 < argc) device = atoi(argv[++i]);
     else if (!strcmp(argv[i], "-batch") && i + 1 < argc) batch = atoi(argv[++i]);
+    else if (!strcmp(argv[i], "-stop-after") && i + 1 < argc) stop_after = atoi(argv[++i]);
   }
   if (ap26_read_state("", KMIN, KMAX, SHIFT, &K, &ITER, &result_hash, &last_trickle,
                       &write_state_a_next)) {
@@ -169,6 +174,8 @@ int main(int argc, char **argv) {
       K_DONE += nk;
       K = kend;
       ITER = 0;
+      searched += nk;
+      if (stop_after > 0 && searched >= stop_after && K <= KMAX) break;
       continue;
     }
     if (ap26_will_search(K)) {
@@ -185,8 +192,19 @@ int main(int argc, char **argv) {
               (int)(time(NULL) - t0), st.device_ms, (long long)st.candidates);
       ITER = 0;
       K_DONE++;
+      searched++;
     }
     K++;
+    if (stop_after > 0 && searched >= stop_after && K <= KMAX) break;
+  }
+  if (K <= KMAX) {                /* stopped early: checkpoint, no hash line */
+    checkpoint(SHIFT, K, 0);
+    if (results_file) fclose(results_file);
+    fprintf(stderr, "Stopped after %d K; resume with the same command.\n", searched);
+    free(aps);
+    free(sols);
+    ap26_destroy(ctx);
+    return EXIT_SUCCESS;
   }
   checkpoint(SHIFT, K, ITER);     /* final, K = KMAX + 1 (AP26.cpp:989) */
   write_hash_line();

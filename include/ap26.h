@@ -57,9 +57,16 @@ typedef struct {
   int32_t use_graphs;     /* 1 = capture per-chunk work in CUDA graphs        */
   int32_t profile;        /* 1 = time every sieve launch with CUDA events
                              (ap26_stats.sieve_ms; disables graph replay)     */
-  int32_t reserved;
+  int32_t cand_ring_log2; /* each of the two candidate rings holds 2^n
+                             entries (default 23; 12..26).  A chunk whose
+                             survivors overflow it is redone with 4x fewer
+                             tiles per launch (at most six times)             */
   int64_t mem_budget;     /* bytes of device memory held by admitted serving
                              units (ap26_serve_submit)                        */
+  double wait_timeout_s;  /* limit of each host wait on the device (default
+                             3600 s); beyond it the call returns
+                             AP26_E_TIMEOUT, and the next call on the context
+                             first waits for the abandoned work to finish     */
 } ap26_opts;
 
 /* One raw report: AP length k, difference multiplier K, first term, and the

@@ -84,3 +84,25 @@ def test_cli_continues_reference_mid_k_checkpoint(tmp_path):
               for f in ("AP26-state.a.txt", "AP26-state.b.txt")]
     assert [str(K), str(K), "0", str(K + 1), "0", "87376"] in states
 
+
+
+def test_cli_stopped_between_k_resumes_to_same_output(tmp_path):
+    """The process ends after each searched K (-stop-after 1: checkpoint of
+    the next K written, no hash line) and is started again until done: the
+    SOL file equals the uninterrupted run's."""
+    kmin, kmax = 366384, 366388          # 366386 = 29 * 12634 is skipped
+    full = tmp_path / "full"
+    full.mkdir()
+    run_cli(full, kmin, kmax, 0)
+    part = tmp_path / "stopped"
+    part.mkdir()
+    runs = 0
+    while True:
+        p = run_cli(part, kmin, kmax, 0, "-stop-after", 1)
+        runs += 1
+        if "Workunit complete" in p.stderr:
+            break
+        assert "Stopped after 1 K" in p.stderr
+        assert runs < 10
+    assert runs == 4                     # 4 searchable K
+    assert (part / "SOL-AP26.txt").read_text() == (full / "SOL-AP26.txt").read_text()

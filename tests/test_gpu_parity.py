@@ -267,3 +267,37 @@ def test_serving_admission_by_memory_budget():
         assert c.serve_submit(2, 1_000_003, 1_000_003, 0) == 0
     finally:
         c.close()
+
+
+# ---- failure paths (host-side: no GPU fault is provoked) --------------------------
+def test_candidate_ring_overflow_is_redone_in_smaller_chunks():
+    """A 2^16-entry candidate ring overflows on a 32768-tile chunk (about
+    2.3 M survivors): the overflow flag makes the host redo the K with 4x
+    fewer tiles per launch until it fits; results are exact."""
+    c = A.Context(0, cand_ring_log2=16)
+    try:
+        aps, st = c.search_k(366384, 0)
+        assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(366384)
+        assert st.error_flags & 1                  # redone in smaller chunks
+        assert st.candidates == 38838420
+        assert c.opts["chunk_tiles"] == 32768      # the setting is restored
+    finally:
+        c.close()
+
+
+def test_wait_deadline_returns_timeout_and_context_recovers():
+    """A host wait longer than wait_timeout_s returns AP26_E_TIMEOUT with the
+    work still queued; the next call waits for it before reusing the host
+    buffers and is exact."""
+    c = A.Context(0, wait_timeout_s=0.005)
+    try:
+        with pytest.raises(A.AP26Error) as e:
+            c.search_k(366384, 0)
+        assert e.value.code == A.E_TIMEOUT
+        c.set_opts(wait_timeout_s=600.0)
+        aps, _ = c.search_k(366384, 0)
+        assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(366384)
+        with pytest.raises(A.AP26Error):
+            A.Context(0, cand_ring_log2=40)
+    finally:
+        c.close()
