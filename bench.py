@@ -12,8 +12,9 @@ search).
 
   value    K/s over all ranks from CUDA-event device time of the pipeline
            (inputs are (K, SHIFT) scalars; nothing to stage)
-  e2e      K/s wall-clock through the C ABI with host buffers, host<->device
-           copies and the host ReportSolution/hash of every report
+  e2e      K/s wall-clock through the C ABI with host buffers: ap26_search_batch
+           (raw reports, result_hash) and ap26_report_batch (SOL lines), with
+           their host<->device copies; ReportSolution runs on the device
   roofline the sieve kernel: algorithmic table bytes (16.62 mean
            consults per shift word x 8 B, oracle-measured) / measured sieve
            launch time, against the measured shared-memory peak
@@ -44,7 +45,7 @@ N59_PER_K = 4808136200          # lattice positions per K (10840 n43 x 443555)
 CONSULTS_PER_WORD = 16.62       # oracle: mean table lookups per shift word (canonical order)
 BYTES_PER_CONSULT = 8
 # H2D/D2H payload per K-job and per call (sizes of the C ABI structures)
-KJOB_BYTES, DEVSTATE_BYTES, APREC_BYTES, COUNT_BYTES = 112, 88, 24, 8
+KJOB_BYTES, DEVSTATE_BYTES, APREC_BYTES, COUNT_BYTES, FINAL_BYTES = 112, 88, 24, 8, 56
 REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 
 
@@ -485,11 +486,17 @@ def main():
 
     seen = {}
 
-    def run_step(i, reporter):
+    def run_step(i, sol_lines):
+        # the public API a host uses for a workunit: ap26_search_batch (raw
+        # reports and the item's result_hash, computed on the device), then
+        # ap26_report_batch for the SOL lines (device-side ReportSolution)
         t0 = time.perf_counter()
         per, res, st = ctx.search_batch(step_items(i))
         for reps in per:
-            reporter.report_all(reps)
+            if reps:
+                rc, fin, _ = ctx.report_batch(reps)
+                assert rc == A.OK, rc
+                sol_lines += [(ln, r[1], fi) for r, f in zip(reps, fin) for ln, fi in f.sols()]
         wall = time.perf_counter() - t0
         local = {}
         for reps in per:
@@ -498,12 +505,12 @@ def main():
         seen.update(local)
         nk = sum(r.ks_searched for r in res)
         naps = sum(r.n_aps for r in res)
-        h2d = KJOB_BYTES * nk + DEVSTATE_BYTES
-        d2h = DEVSTATE_BYTES + COUNT_BYTES * nk + APREC_BYTES * naps
+        h2d = KJOB_BYTES * nk + DEVSTATE_BYTES + APREC_BYTES * naps
+        d2h = DEVSTATE_BYTES + 2 * COUNT_BYTES * nk + (APREC_BYTES + FINAL_BYTES) * naps
         return st, wall, nk, h2d, d2h
 
     for i in range(args.warmup):
-        run_step(i, A.Reporter())
+        run_step(i, [])
     seen.clear()
 
     def barrier():
@@ -511,7 +518,7 @@ def main():
         if world > 1:
             dist.barrier()
 
-    rep = A.Reporter()
+    rep = []
     tot = {"dev_ms": 0.0, "sieve_ms": 0.0, "cells": 0, "launches": 0, "ks": 0, "h2d": 0,
            "d2h": 0, "kernels": 0, "cand": 0}
     barrier()
@@ -589,7 +596,8 @@ def main():
             "e2e": {"value": ks_total / wall_max, "unit": "K/s",
                     "h2d_bytes_per_step": tot["h2d"] // args.steps,
                     "d2h_bytes_per_step": tot["d2h"] // args.steps,
-                    "includes": "C-ABI call, job H2D, report D2H, host ReportSolution/hash"},
+                    "includes": "C-ABI calls (ap26_search_batch + ap26_report_batch), job "
+                                "H2D, report/result D2H, device-side ReportSolution and hash"},
             "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_gbs,
                          "unit": "GB/s", "frac": achieved / smem_gbs,
                          "traffic": traffic,
