@@ -310,6 +310,20 @@ static int cuda_fail(ap26_ctx *ctx, cudaError_t e, const char *what) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
+// Device buffer owned by one call of a kernel-level entry point: freed on
+// every return path, the early CUDA-error returns of CK included.
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * n); }
+};
+
 extern "C" int ap26_version(void) { return 10000; }
 
 extern "C" const char *ap26_strerror(int code) {
@@ -379,9 +393,16 @@ static int ensure_jobs(ap26_ctx *ctx, int njobs) {
   const int64_t need = (int64_t)cap * (sizeof(KJob) + TABLE_WORDS * 4 + 8);
   if (cap > 64 && need > ctx->opts.mem_budget) return AP26_E_NOMEM;
   if (ctx->d_jobs) {
+    drain(ctx);
     cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
     cudaFree(ctx->d_job_hash);
     cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts); cudaFreeHost(ctx->h_job_hash);
+    // cleared first: a failed allocation below must not leave freed pointers
+    // for ap26_destroy to free again
+    ctx->d_jobs = nullptr; ctx->d_tables = nullptr; ctx->d_job_counts = nullptr;
+    ctx->d_job_hash = nullptr;
+    ctx->h_jobs = nullptr; ctx->h_job_counts = nullptr; ctx->h_job_hash = nullptr;
+    ctx->jobs_cap = 0;
   }
   CK(cudaMalloc(&ctx->d_jobs, sizeof(KJob) * cap));
   CK(cudaMalloc(&ctx->d_tables, sizeof(uint32_t) * TABLE_WORDS * (size_t)cap));
@@ -1139,21 +1160,22 @@ extern "C" int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count, 
   if (!ctx || !N || !verdict || count < 0) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   if (count == 0) return AP26_OK;
-  uint64_t *dN = nullptr;
-  uint8_t *dV = nullptr;
-  unsigned long long *dsq = nullptr, hsq = 0;
-  CK(cudaMalloc(&dN, sizeof(uint64_t) * count));
-  CK(cudaMalloc(&dV, count));
-  CK(cudaMalloc(&dsq, sizeof(unsigned long long)));
+  DevBuf<uint64_t> dN;
+  DevBuf<uint8_t> dV;
+  DevBuf<unsigned long long> dsq;
+  unsigned long long hsq = 0;
+  CK(dN.alloc(count));
+  CK(dV.alloc(count));
+  CK(dsq.alloc(1));
   cudaStream_t s = ctx->stream;
-  CK(cudaMemsetAsync(dsq, 0, sizeof(unsigned long long), s));
-  CK(cudaMemcpyAsync(dN, N, sizeof(uint64_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(dsq.p, 0, sizeof(unsigned long long), s));
+  CK(cudaMemcpyAsync(dN.p, N, sizeof(uint64_t) * count, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev0, s));
-  sprp_batch_kernel<<<ctx->num_sms * 16, 256, 0, s>>>(dN, count, dV, dsq);
+  sprp_batch_kernel<<<ctx->num_sms * 16, 256, 0, s>>>(dN.p, count, dV.p, dsq.p);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
-  CK(cudaMemcpyAsync(verdict, dV, count, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(&hsq, dsq, sizeof(hsq), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(verdict, dV.p, count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&hsq, dsq.p, sizeof(hsq), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -1164,7 +1186,6 @@ extern "C" int ap26_sprp_batch(ap26_ctx *ctx, const uint64_t *N, int64_t count, 
     stats->late_items = (int64_t)hsq;   // modular squarings performed
     stats->launches = 1;
   }
-  cudaFree(dN); cudaFree(dV); cudaFree(dsq);
   return AP26_OK;
 }
 
@@ -1175,20 +1196,20 @@ extern "C" int ap26_sprp_bases(ap26_ctx *ctx, const uint64_t *N, const uint32_t 
     if (a[i] < 2 || a[i] > 31) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   if (count == 0) return AP26_OK;
-  uint64_t *dN = nullptr;
-  uint32_t *dA = nullptr;
-  uint8_t *dV = nullptr;
-  CK(cudaMalloc(&dN, sizeof(uint64_t) * count));
-  CK(cudaMalloc(&dA, sizeof(uint32_t) * count));
-  CK(cudaMalloc(&dV, count));
+  DevBuf<uint64_t> dN;
+  DevBuf<uint32_t> dA;
+  DevBuf<uint8_t> dV;
+  CK(dN.alloc(count));
+  CK(dA.alloc(count));
+  CK(dV.alloc(count));
   cudaStream_t s = ctx->stream;
-  CK(cudaMemcpyAsync(dN, N, sizeof(uint64_t) * count, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(dA, a, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dN.p, N, sizeof(uint64_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dA.p, a, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev0, s));
-  sprp_bases_kernel<<<ctx->num_sms * 16, 256, 0, s>>>(dN, dA, count, dV);
+  sprp_bases_kernel<<<ctx->num_sms * 16, 256, 0, s>>>(dN.p, dA.p, count, dV.p);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
-  CK(cudaMemcpyAsync(verdict, dV, count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(verdict, dV.p, count, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -1198,7 +1219,6 @@ extern "C" int ap26_sprp_bases(ap26_ctx *ctx, const uint64_t *N, const uint32_t 
     stats->device_ms = ms;
     stats->launches = 1;
   }
-  cudaFree(dN); cudaFree(dA); cudaFree(dV);
   return AP26_OK;
 }
 
@@ -1209,26 +1229,26 @@ extern "C" int ap26_report_batch(ap26_ctx *ctx, const ap26_ap *raw, int64_t n, a
   CK(cudaSetDevice(ctx->device));
   if (stats) memset(stats, 0, sizeof(*stats));
   if (n == 0) return AP26_OK;
-  APRec *dR = nullptr;
-  FinRec *dF = nullptr;
-  CK(cudaMalloc(&dR, sizeof(APRec) * n));
-  CK(cudaMalloc(&dF, sizeof(FinRec) * n));
+  DevBuf<APRec> dR;
+  DevBuf<FinRec> dF;
+  CK(dR.alloc(n));
+  CK(dF.alloc(n));
   cudaStream_t s = ctx->stream;
   // ap26_ap and APRec share a layout; with jobs == null the job field is K
-  CK(cudaMemcpyAsync(dR, raw, sizeof(APRec) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dR.p, raw, sizeof(APRec) * n, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev0, s));
   ReportArgs ra;
-  ra.aps = dR;
+  ra.aps = dR.p;
   ra.count = nullptr;
   ra.n = n;
   ra.jobs = nullptr;
-  ra.fin = dF;
+  ra.fin = dF.p;
   ra.job_hash = nullptr;
   const long long want = (n + REPORT_WARPS - 1) / REPORT_WARPS;
   report_kernel<<<(int)std::min<long long>(want, ctx->num_sms * 8), REPORT_WARPS * 32, 0, s>>>(ra);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
-  CK(cudaMemcpyAsync(out, dF, sizeof(FinRec) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(out, dF.p, sizeof(FinRec) * n, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -1237,7 +1257,6 @@ extern "C" int ap26_report_batch(ap26_ctx *ctx, const ap26_ap *raw, int64_t n, a
     stats->device_ms = ms;
     stats->launches = 1;
   }
-  cudaFree(dR); cudaFree(dF);
   unsigned long long add = 0;
   for (int64_t i = 0; i < n; i++) {
     if (out[i].status != AP26_OK) return out[i].status;
@@ -1255,23 +1274,24 @@ extern "C" int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t 
   drain(ctx);
   if (count == 0) return AP26_OK;
   fill_job(ctx->h_jobs[0], K, 0, 0, 0, 0);
-  int64_t *dn = nullptr, *df = nullptr;
-  int32_t *dk = nullptr;
-  CK(cudaMalloc(&dn, sizeof(int64_t) * count));
-  CK(cudaMalloc(&df, sizeof(int64_t) * count));
-  CK(cudaMalloc(&dk, sizeof(int32_t) * count));
+  DevBuf<int64_t> dn, df;
+  DevBuf<int32_t> dk;
+  CK(dn.alloc(count));
+  CK(df.alloc(count));
+  CK(dk.alloc(count));
   cudaStream_t s = ctx->stream;
   memset(ctx->h_st, 0, sizeof(DevState));
   CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
   setup_jobs_kernel<<<1, 256, 0, s>>>(ctx->d_jobs, 1, ctx->d_tables);
-  CK(cudaMemcpyAsync(dn, n, sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dn.p, n, sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev0, s));
-  chain_explicit_kernel<<<ctx->num_sms * 8, 128, 0, s>>>(ctx->d_jobs, dn, count, dk, df, ctx->d_st);
+  chain_explicit_kernel<<<ctx->num_sms * 8, 128, 0, s>>>(ctx->d_jobs, dn.p, count, dk.p, df.p,
+                                                         ctx->d_st);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
-  CK(cudaMemcpyAsync(k_out, dk, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(first_out, df, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(k_out, dk.p, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(first_out, df.p, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   float ms = 0;
@@ -1282,22 +1302,23 @@ extern "C" int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t 
     stats->error_flags = (int32_t)ctx->h_st->err_flags;
     stats->launches = 2;
   }
-  cudaFree(dn); cudaFree(df); cudaFree(dk);
   return (ctx->h_st->err_flags & ERR_DOMAIN) ? AP26_E_DOMAIN : AP26_OK;
 }
 
 extern "C" int ap26_probe_peaks(ap26_ctx *ctx, double *smem_gbs, double *int_tops) {
   if (!ctx) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  unsigned *sink = nullptr;
-  CK(cudaMalloc(&sink, sizeof(unsigned)));
+  drain(ctx);
+  DevBuf<unsigned> sink;
+  CK(sink.alloc(1));
   cudaStream_t s = ctx->stream;
   const int blocks = ctx->num_sms * 4, threads = 256;
   const int siters = 4096, iiters = 4096;
   float ms = 0;
   for (int rep = 0; rep < 2; rep++) {
     CK(cudaEventRecord(ctx->ev0, s));
-    smem_probe_kernel<<<blocks, threads, 0, s>>>(siters, sink);
+    smem_probe_kernel<<<blocks, threads, 0, s>>>(siters, sink.p);
+    CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev1, s));
     CK(cudaEventSynchronize(ctx->ev1));
   }
@@ -1305,14 +1326,14 @@ extern "C" int ap26_probe_peaks(ap26_ctx *ctx, double *smem_gbs, double *int_top
   if (smem_gbs) *smem_gbs = (double)blocks * threads * siters * 8 * 16 / (ms * 1e-3) / 1e9;
   for (int rep = 0; rep < 2; rep++) {
     CK(cudaEventRecord(ctx->ev0, s));
-    int_probe_kernel<<<blocks, threads, 0, s>>>(iiters, sink);
+    int_probe_kernel<<<blocks, threads, 0, s>>>(iiters, sink.p);
+    CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev1, s));
     CK(cudaEventSynchronize(ctx->ev1));
   }
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   // one IMAD (a*m + c) per element per step: 8 * 16 per iteration
   if (int_tops) *int_tops = (double)blocks * threads * iiters * 8 * 16 / (ms * 1e-3) / 1e12;
-  cudaFree(sink);
   return AP26_OK;
 }
 
