@@ -575,10 +575,10 @@ def main():
         cells_per_launch = tot["cells"] / max(1, tot["launches"])
         alg_bytes = cells_per_launch * CONSULTS_PER_WORD * BYTES_PER_CONSULT
         achieved = alg_bytes / (sieve_launch_ms / 1000.0) / 1e9
-        # DRAM traffic of one sieve launch, scaled from the committed ncu capture
-        # (profiles/sieve_kernel_ncu.md: 74.0 KB for a 8385-tile launch).
-        chunk_tiles = ctx.opts["chunk_tiles"]
-        traffic = 74.0e3 * (tot["cells"] / max(1, tot["launches"])) / (8385 * 256 * 350)
+        # DRAM traffic of one sieve launch, scaled by cells from the committed
+        # ncu capture (profiles/sieve_kernel_ncu.md: 69.4 KB read + 2.8 KB
+        # written by an 8385-tile launch of the default variant)
+        traffic = 72.2e3 * (tot["cells"] / max(1, tot["launches"])) / (8385 * 256 * 350)
         line = {
             "metric": "K/s, 10-shift search", "value": ks_total / (dev_ms / 1000.0),
             "unit": "K/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

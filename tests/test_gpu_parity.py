@@ -191,12 +191,19 @@ def test_recorded_reference_ranges(ctx):
     """Every K with a recorded reference raw-report file, at every recorded
     SHIFT (0, and 640 / 1280 / 15360 for seeded K): device reports equal
     the reference's, in order."""
+    import json
     cases = recorded_reference_ks()
     assert len(cases) >= 3 and len({s for _, s in cases}) >= 1
+    # whole-K survivor counts at nonzero SHIFT (tests/golden/make_shift_counts.py)
+    pinned = {(p["K"], p["shift"]): p["candidates"]
+              for p in json.load(open(os.path.join(GOLDEN, "shift_counts.json")))}
+    assert len(pinned) >= 6
     for K, shift in cases:
         aps, st = ctx.search_k(K, shift)
         assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(K, shift), (K, shift)
         assert st.error_flags == 0
+        if (K, shift) in pinned:
+            assert st.candidates == pinned[(K, shift)], (K, shift)
 
 
 def test_search_k_rejects_unsearchable_and_out_of_domain(ctx):
