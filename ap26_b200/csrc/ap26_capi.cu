@@ -237,15 +237,37 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 using namespace ap26;
 
 // ---- context --------------------------------------------------------------------
+// A serving unit's running state, kept on the device in the unit's slot:
+// the partial ReportSolution hash sum, survivor count and K-jobs finished.
+struct UnitState {
+  unsigned long long hash_add;
+  unsigned long long candidates;
+  int32_t ks_done;
+  int32_t pad;
+};
+constexpr int kUnitSlots = 1024;
+
+// After a serving slice: each K-job's survivor count and ReportSolution hash
+// sum go into its unit's slot (KJob::item holds the slot).
+__global__ void unit_accumulate_kernel(const KJob *jobs, int njobs,
+                                       const unsigned long long *job_counts,
+                                       const unsigned long long *job_hash, UnitState *units) {
+  for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
+    UnitState &u = units[jobs[j].item];
+    atomicAdd(&u.hash_add, job_hash[j]);
+    atomicAdd(&u.candidates, job_counts[j]);
+    atomicAdd(&u.ks_done, 1);
+  }
+}
+
 struct ServeUnit {
   ap26_item item;
   std::vector<int> ks;           // searchable K of the unit
   size_t next_k = 0;             // next K to put on the device
   int inflight = 0;              // K-jobs of this unit in the current slice
-  int done_k = 0;
+  int done_k = 0;                // host copy of the count, for scheduling
+  int slot = -1;                 // its UnitState on the device
   std::vector<ap26_ap> aps;
-  int64_t candidates = 0;
-  unsigned long long hash_add = 0;   // device-side ReportSolution hash sum
   int status = AP26_OK;
   std::chrono::steady_clock::time_point t_submit;
   double latency_ms = 0;
@@ -286,6 +308,8 @@ struct ap26_ctx {
   std::deque<ServeUnit> units;
   std::deque<ServeUnit> finished;
   int64_t bytes_in_use = 0;     // device bytes held by admitted serving units
+  UnitState *d_units = nullptr; // kUnitSlots serving-unit states
+  std::vector<int> free_slots;
   std::string last_error;
   bool pending = false;        // a call timed out with its work still queued
 };
@@ -468,6 +492,8 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
       CKC(cudaEventCreateWithFlags(&ctx->chain_done[r], cudaEventDisableTiming));
     }
     CKC(cudaMalloc(&ctx->d_aps, sizeof(APRec) * ctx->ap_cap));
+    CKC(cudaMalloc(&ctx->d_units, sizeof(UnitState) * kUnitSlots));
+    for (int i = kUnitSlots - 1; i >= 0; i--) ctx->free_slots.push_back(i);
     CKC(cudaMalloc(&ctx->d_fin, sizeof(FinRec) * ctx->ap_cap));
     CKC(cudaMallocHost(&ctx->h_fin, sizeof(FinRec) * ctx->ap_cap));
     CKC(cudaMallocHost(&ctx->h_st, sizeof(DevState)));
@@ -493,7 +519,7 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
   for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
   cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
-  cudaFree(ctx->d_job_hash); cudaFree(ctx->d_fin);
+  cudaFree(ctx->d_job_hash); cudaFree(ctx->d_fin); cudaFree(ctx->d_units);
   cudaFreeHost(ctx->h_job_hash); cudaFreeHost(ctx->h_fin);
   cudaFree(ctx->d_st); cudaFree(ctx->d_cand[0]); cudaFree(ctx->d_cand[1]); cudaFree(ctx->d_aps);
   for (int r = 0; r < 2; r++) {
@@ -979,7 +1005,12 @@ extern "C" int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item) {
   for (int K = item->kmin; K <= item->kmax; K++)
     if (ap26_will_search(K)) u.ks.push_back(K);
   const int64_t need = unit_bytes(u.ks.size());
-  if (ctx->bytes_in_use + need > ctx->opts.mem_budget) return AP26_E_NOMEM;
+  if (ctx->bytes_in_use + need > ctx->opts.mem_budget || ctx->free_slots.empty())
+    return AP26_E_NOMEM;
+  CK(cudaSetDevice(ctx->device));
+  u.slot = ctx->free_slots.back();
+  CK(cudaMemsetAsync(ctx->d_units + u.slot, 0, sizeof(UnitState), ctx->stream));
+  ctx->free_slots.pop_back();
   ctx->bytes_in_use += need;
   u.t_submit = std::chrono::steady_clock::now();
   ctx->units.push_back(std::move(u));
@@ -1012,14 +1043,19 @@ extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
     int rc;
     if ((rc = ensure_jobs(ctx, (int)picked.size())) != AP26_OK) return rc;
     for (size_t j = 0; j < picked.size(); j++)
-      fill_job(ctx->h_jobs[j], picked[j].second, picked[j].first->item.shift, (int)j, 0,
-               N53_PER_K);
+      fill_job(ctx->h_jobs[j], picked[j].second, picked[j].first->item.shift,
+               picked[j].first->slot, 0, N53_PER_K);
     long long n = 0;
     ap26_stats st;
     rc = run_jobs_retry(ctx, (int)picked.size(), false, &st, &n, true);
     if (rc != AP26_OK) {
       for (auto &pk : picked) pk.first->status = rc;
     } else {
+      // the units' running sums stay on the device
+      unit_accumulate_kernel<<<1, 256, 0, ctx->stream>>>(ctx->d_jobs, (int)picked.size(),
+                                                         ctx->d_job_counts, ctx->d_job_hash,
+                                                         ctx->d_units);
+      CK(cudaGetLastError());
       std::vector<std::vector<RepOut>> per_job(picked.size());
       for (auto &r : collect_reports(ctx, n)) per_job[r.first].push_back(r.second);
       for (size_t j = 0; j < picked.size(); j++) {
@@ -1029,8 +1065,6 @@ extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
           u->aps.push_back(r.ap);
           if (r.fin.status != AP26_OK && u->status == AP26_OK) u->status = r.fin.status;
         }
-        u->candidates += (int64_t)ctx->h_job_counts[j];
-        u->hash_add += ctx->h_job_hash[j];
         u->done_k++;
       }
     }
@@ -1057,15 +1091,26 @@ extern "C" int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *ap
   ServeUnit &u = ctx->finished.front();
   *n_aps = (int64_t)u.aps.size();
   if ((int64_t)u.aps.size() > ap_cap) return AP26_E_CAPACITY;
+  CK(cudaSetDevice(ctx->device));
+  drain(ctx);
+  UnitState us;
+  CK(cudaMemcpyAsync(&us, ctx->d_units + u.slot, sizeof(us), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   if (!u.aps.empty()) memcpy(aps, u.aps.data(), sizeof(ap26_ap) * u.aps.size());
   res->id = u.item.id;
   res->status = u.status;
+  if (res->status == AP26_OK && us.ks_done != u.done_k) {
+    res->status = AP26_E_CUDA;       // the device record disagrees with the schedule
+    ctx->last_error = "serving unit state on the device is inconsistent";
+  }
   res->n_aps = (int32_t)u.aps.size();
   res->first_ap = 0;
-  res->candidates = u.candidates;
+  res->candidates = (int64_t)us.candidates;
   res->ks_searched = (int32_t)u.ks.size();
-  res->result_hash = hash_fold(0, u.hash_add);
+  res->result_hash = hash_fold(0, us.hash_add);
   res->latency_ms = u.latency_ms;
+  ctx->free_slots.push_back(u.slot);
   ctx->finished.pop_front();
   return 1;
 }

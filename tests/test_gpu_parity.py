@@ -308,3 +308,22 @@ def test_wait_deadline_returns_timeout_and_context_recovers():
             A.Context(0, cand_ring_log2=40)
     finally:
         c.close()
+
+
+def test_cuda_graph_replay_is_exact():
+    """The plain form with its per-chunk sequence (chunk_begin -> sieve ->
+    chain -> chunk_end) captured once in a CUDA graph and replayed for
+    every chunk: same reports as the reference, for two K in a row (one
+    graph reused) and for the count-only form (its own graph)."""
+    c = A.Context(0, use_graphs=1, profile=0)
+    try:
+        for K in (366384, 44121555):
+            aps, st = c.search_k(K, 0)
+            assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(K), K
+            assert st.error_flags == 0
+        counts, _ = c.sieve_count([366384], 0)
+        assert counts[0] == 38838420
+        aps, _ = c.search_k(47715109, 0)
+        assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(47715109)
+    finally:
+        c.close()
