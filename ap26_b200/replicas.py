@@ -1,6 +1,6 @@
 """Multi-GPU form of the search: independent replicas over disjoint K ranges.
 
-The per-K search has no exchange step (SURVEY: K values are independent), so
+The per-K search has no exchange step (every K is searched independently), so
 N GPUs run N replicas, each on its own K range, with no collective on the
 data path.  The only cross-rank steps are host-side: the partial result
 hashes are combined (the reference's result hash is an additive sum reduced
