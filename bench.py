@@ -496,6 +496,7 @@ def main():
             if reps:
                 rc, fin, _ = ctx.report_batch(reps)
                 assert rc == A.OK, rc
+                st.launches += 1          # its report_kernel
                 sol_lines += [(ln, r[1], fi) for r, f in zip(reps, fin) for ln, fi in f.sols()]
         wall = time.perf_counter() - t0
         local = {}
