@@ -106,3 +106,28 @@ def test_cli_stopped_between_k_resumes_to_same_output(tmp_path):
         assert runs < 10
     assert runs == 4                     # 4 searchable K
     assert (part / "SOL-AP26.txt").read_text() == (full / "SOL-AP26.txt").read_text()
+
+
+def test_cli_whole_64k_workunit_matches_reference(tmp_path, oracle):
+    """The bench's 64-K workunit (KMIN 43241056, SHIFT 0; 51 searchable K)
+    through the command in batched mode: SOL lines and hash equal the
+    reference's ReportSolution over its own raw reports of every K
+    (tests/golden/ref_raw/shift0), in K order."""
+    import ctypes
+    kmin, kmax = 43241056, 43241056 + 63
+    h = ctypes.c_int(0)
+    sol = ctypes.create_string_buffer(1 << 16)
+    n = 0
+    for K in range(kmin, kmax + 1):
+        if not A.will_search(K):
+            continue
+        n += 1
+        for k, KK, first in ref_raw(K):
+            assert oracle.ao_report(ctypes.byref(h), k, KK, ctypes.c_int64(first), sol,
+                                    len(sol)) == 0
+    assert n == 51
+    hexb = ctypes.create_string_buffer(17)
+    oracle.ao_hash_hex(kmin, kmax, h, hexb)
+    expected = sol.value.decode() + hexb.value.decode() + "\n"
+    run_cli(tmp_path, kmin, kmax, 0, "-batch", 16)
+    assert (tmp_path / "SOL-AP26.txt").read_text() == expected
