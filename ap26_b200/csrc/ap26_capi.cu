@@ -675,8 +675,11 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     ctx->graph_key = key;
   }
   const bool prof = ctx->opts.profile != 0;
-  if (prof && (int)ctx->prof_events.size() < 2 * (int)nchunks) {
-    for (int i = (int)ctx->prof_events.size(); i < 2 * (int)nchunks; i++) {
+  // sieve launches timed with events: the first kProfChunks chunks at most
+  constexpr unsigned long long kProfChunks = 4096;
+  const unsigned long long nprof = prof ? std::min(nchunks, kProfChunks) : 0;
+  if ((unsigned long long)ctx->prof_events.size() < 2 * nprof) {
+    for (size_t i = ctx->prof_events.size(); i < 2 * nprof; i++) {
       cudaEvent_t e;
       CK(cudaEventCreate(&e));
       ctx->prof_events.push_back(e);
@@ -690,9 +693,9 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
       // ring r is free once the chain walk of chunk c-2 has read it
       if (two_streams && c >= 2) CK(cudaStreamWaitEvent(s, ctx->chain_done[r], 0));
       chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st, r);
-      if (prof) CK(cudaEventRecord(ctx->prof_events[2 * c], s));
+      if (c < nprof) CK(cudaEventRecord(ctx->prof_events[2 * c], s));
       V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa[r]);
-      if (prof) CK(cudaEventRecord(ctx->prof_events[2 * c + 1], s));
+      if (c < nprof) CK(cudaEventRecord(ctx->prof_events[2 * c + 1], s));
       if (two_streams) {
         chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap, r);
         CK(cudaEventRecord(ctx->sieve_done[r], s));
@@ -756,8 +759,14 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     stats->sieve_cells = n53 * J59 * WORDS;
     stats->sieve_launches = (int32_t)nchunks;
     if (prof) {
+      if (nprof < nchunks) {
+        // only the first nprof chunks were timed; all of them are full
+        stats->sieve_cells = (int64_t)(nprof * (unsigned long long)ctx->opts.chunk_tiles) *
+                             tile_n53 * J59 * WORDS;
+        stats->sieve_launches = (int32_t)nprof;
+      }
       double sm = 0;
-      for (unsigned long long c = 0; c < nchunks; c++) {
+      for (unsigned long long c = 0; c < nprof; c++) {
         float t = 0;
         cudaEventElapsedTime(&t, ctx->prof_events[2 * c], ctx->prof_events[2 * c + 1]);
         sm += t;
