@@ -14,6 +14,9 @@
 //                       generated from a flat index)
 //   chain_kernel        base-2 SPRP chain walk (replaces checkn.cl)
 //   chunk_end_kernel    advances the chunk window
+//   report_kernel       after the last chunk: ReportSolution of every raw
+//                       report (9-base validation, split recursion, hash;
+//                       src/common/AP26.cpp:484-602), per-job hash sums
 //
 // ---------------------------------------------------------------------------
 // Sieve formulation.  The reference ANDs, for every lattice value n59 and
