@@ -29,6 +29,8 @@ N53_PER_K = 137375320
 N59_PER_K = 4808136200
 MOD = 258559632607830
 PRIM23 = 223092870
+KMAX_SAFE = 400_000_000       # AP26_KMAX_SAFE
+SHIFT_MAX = 16000             # AP26_SHIFT_MAX
 
 
 class Opts(ctypes.Structure):

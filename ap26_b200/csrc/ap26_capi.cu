@@ -1446,13 +1446,18 @@ struct NoallocScratch {
   unsigned long long counts[AP26_NOALLOC_MAX_K];
   uint32_t tables[AP26_NOALLOC_MAX_K][TABLE_WORDS];
 };
+static_assert(sizeof(NoallocScratch) == AP26_NOALLOC_SCRATCH_BYTES,
+              "the scratch size stated in ap26.h");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
 
 // Fills the job descriptors and zeroes the counters and state left behind by
 // the previous call (the array keeps the last call's contents).  A K outside
-// [1, AP26_KMAX_SAFE] gets an empty lattice range and a count of -1.
+// [1, AP26_KMAX_SAFE] gets an empty lattice range, no tiles and a count of
+// -1, so it costs the sieve nothing; the tile prefix skips it (find_job takes
+// the last job whose first tile is <= the tile, which is never an empty one).
 __global__ void noalloc_init_kernel(NoallocScratch *s, const int32_t *Ks, int nK, int shift,
                                     int tile_n53) {
+  __shared__ int32_t s_tiles[AP26_NOALLOC_MAX_K];
   const int j = threadIdx.x;
   const int64_t ntiles = (N53_PER_K + tile_n53 - 1) / tile_n53;
   if (j < nK) {
@@ -1465,14 +1470,22 @@ __global__ void noalloc_init_kernel(NoallocScratch *s, const int32_t *Ks, int nK
     J.item = ok ? 0 : -1;
     J.q_begin = 0;
     J.q_end = ok ? N53_PER_K : 0;
-    J.ntiles = (int32_t)ntiles;
-    J.tile_begin = (int64_t)j * ntiles;
+    J.ntiles = ok ? (int32_t)ntiles : 0;
+    s_tiles[j] = J.ntiles;
     s->counts[j] = 0;
   }
+  __syncthreads();
+  if (j < nK) {
+    int64_t begin = 0;
+    for (int i = 0; i < j; i++) begin += s_tiles[i];
+    s->jobs[j].tile_begin = begin;
+  }
   if (j == 0) {
+    int64_t total = 0;
+    for (int i = 0; i < nK; i++) total += s_tiles[i];
     memset(&s->st, 0, sizeof(DevState));
-    s->st.chunk_size = (unsigned long long)ntiles * nK;
-    s->st.total_tiles = (unsigned long long)ntiles * nK;
+    s->st.chunk_size = (unsigned long long)total;
+    s->st.total_tiles = (unsigned long long)total;
   }
 }
 
@@ -1523,11 +1536,22 @@ static int noalloc_setup(int device, NoallocDevice **out) {
 }
 }  // namespace ap26
 
+// A launch error raised by this entry point's own launches: taken (and so
+// cleared) here.  An error already pending before the first launch belongs
+// to the caller's earlier work and is left untouched: the call returns
+// AP26_E_CUDA without launching anything.
+static bool noalloc_launch_failed() {
+  if (cudaPeekAtLastError() == cudaSuccess) return false;
+  cudaGetLastError();
+  return true;
+}
+
 extern "C" int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
                                         int64_t *d_counts, void *stream) {
   if (!d_Ks || !d_counts || nK < 1 || device < 0 || device >= 64) return AP26_E_ARG;
   if (nK > AP26_NOALLOC_MAX_K) return AP26_E_CAPACITY;
   if (shift < 0 || shift > AP26_SHIFT_MAX) return AP26_E_DOMAIN;
+  if (cudaPeekAtLastError() != cudaSuccess) return AP26_E_CUDA;
   int prev = 0;
   if (cudaGetDevice(&prev) != cudaSuccess) return AP26_E_CUDA;
   if (prev != device && cudaSetDevice(device) != cudaSuccess) return AP26_E_CUDA;
@@ -1537,14 +1561,20 @@ extern "C" int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK,
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const SieveVariant &V = kVariants[0];
     NoallocScratch *S = d->ptr;
-    noalloc_init_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, d_Ks, nK, shift, V.WARPS * 32);
-    setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0]);
-    chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st, 0);
-    const SieveArgs sa = sieve_args(S->jobs, nK, &S->tables[0][0], &S->st, nullptr, 0,
-                                    S->counts, 1, &S->st.cand_count[0]);
-    V.kernel<<<d->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
-    noalloc_finish_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, nK, d_counts);
-    if (cudaGetLastError() != cudaSuccess) rc = AP26_E_CUDA;
+    do {
+      noalloc_init_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, d_Ks, nK, shift, V.WARPS * 32);
+      if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
+      setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0]);
+      if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
+      chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st, 0);
+      if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
+      const SieveArgs sa = sieve_args(S->jobs, nK, &S->tables[0][0], &S->st, nullptr, 0,
+                                      S->counts, 1, &S->st.cand_count[0]);
+      V.kernel<<<d->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+      if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
+      noalloc_finish_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, nK, d_counts);
+      if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
+    } while (0);
   }
   if (prev != device) cudaSetDevice(prev);
   return rc;

@@ -2,8 +2,8 @@
 //
 // The numeric constants are the reference's (ibethune/ap26,
 // src/common/CONST.H:7-27); the per-prime parameters below are derived from
-// them at compile time for the B200 sieve formulation described in
-// ap26_sieve.cuh.
+// them at compile time for the bitstring-window sieve formulation described
+// at the top of ap26_kernels.cuh.
 #pragma once
 #include <stdint.h>
 
@@ -50,7 +50,7 @@ constexpr int word_offset(int g) {
   for (int i = 0; i < g; i++) o += nwords(PRIMES[i]);
   return o;
 }
-constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2566 words, 10264 bytes
+constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2568 words, 10272 bytes
 
 constexpr int64_t mod_pos(int64_t a, int64_t m) { return ((a % m) + m) % m; }
 constexpr int inv_mod(int a, int p) {                // a^-1 mod p, p prime
@@ -86,7 +86,7 @@ constexpr PrimeParam make_param(int g) {
   return PrimeParam{p, A, B, C, k, word_offset(g), (uint32_t)M};
 }
 
-// Residue 0 test helpers for the 7..23 filter (sieve.cl:333-346,
+// Residue 0 test helpers for the 7..23 filter (sieve.cl:123-142,
 // cpusse2.cpp:563-568).
 constexpr int SMALL_PRIMES[6] = {7, 11, 13, 17, 19, 23};
 

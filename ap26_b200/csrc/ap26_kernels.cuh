@@ -21,7 +21,7 @@
 // ---------------------------------------------------------------------------
 // Sieve formulation.  The reference ANDs, for every lattice value n59 and
 // every shift word w (absolute shift SHIFT+64w), the 83 table words
-// OKOK_{p,w}[n59 mod p] (sieve.cl:238-320), where bit b of OKOK_{p,w}[r] is
+// OKOK_{p,w}[n59 mod p] (sieve.cl:28-113), where bit b of OKOK_{p,w}[r] is
 // OK_p[(r + (SHIFT+64w+b)*MOD) mod p] (setupokok.cl, cpusse2.cpp:38-43).
 // Multiplying the index by MOD^-1 mod p turns the 640 bits of all 10 words
 // into ONE window of a p-periodic bitstring:
@@ -39,7 +39,7 @@
 //                lanes on the same prime, until stage SL
 //   late         pairs alive at SL wait in a second per-warp queue until
 //                enough have gathered to go through primes SL..82 together;
-//                surviving bits pass the 7..23 filter (sieve.cl:333-346) and
+//                surviving bits pass the 7..23 filter (sieve.cl:123-142) and
 //                become candidates n = n59 + (SHIFT + 64w + b) * MOD.
 #pragma once
 #include <stdint.h>

@@ -346,6 +346,51 @@ def _mixed_items(rng, n, max_len, shifts=(0, 640, 1280)):
     return items
 
 
+# ---- the seeded workloads of the secondary bench keys ------------------------------
+# Each is a stated prefix of its full-size configuration, sized so that the
+# whole default run stays within a few minutes; tests/golden/make_golden.py
+# records the reference's own raw reports and survivor counts for every
+# (K, SHIFT) they contain.
+BATCHED_FULL_ITEMS = 4096      # the full batched configuration: 4096 items ...
+BATCHED_MAX_LEN = 64           # ... of log-uniform length 1..64 K
+BATCHED_ITEMS = 5              # bench prefix: the first 5 items (20 searchable K)
+SERVE_UNITS, SERVE_MAX_K = 32, 8
+SIEVE_PAIR_KMIN = 27872096     # default_rng(31).integers(1e6, 5e7 - 1024): 1024 K at SHIFT 640
+SIEVE_PAIR_FULL, SIEVE_PAIR_K, SIEVE_PAIR_PINNED, SIEVE_PAIR_SHIFT = 1024, 64, 16, 640
+
+
+def batched_items(n=BATCHED_ITEMS):
+    """The first n of the 4096 seeded mixed work items (seed 44)."""
+    import numpy as np
+    return _mixed_items(np.random.default_rng(44), BATCHED_FULL_ITEMS, BATCHED_MAX_LEN)[:n]
+
+
+def serve_units(n=SERVE_UNITS, max_k=SERVE_MAX_K):
+    """Seeded serving units (seed 55): log-uniform 1..max_k K, mixed SHIFT."""
+    import numpy as np
+    return _mixed_items(np.random.default_rng(55), n, max_k)
+
+
+def sieve_pair_ks(n=SIEVE_PAIR_K):
+    """The first n K of the 1024 consecutive K of the sieve roofline pair."""
+    return list(range(SIEVE_PAIR_KMIN, SIEVE_PAIR_KMIN + n))
+
+
+def fixture_pairs():
+    """Every (K, SHIFT) of the secondary workloads whose reference results are
+    recorded: the first 16 searchable K of the sieve pair, then the batched
+    and serving items' searchable K."""
+    out = [(k, SIEVE_PAIR_SHIFT) for k in sieve_pair_ks() if will_search(k)][:SIEVE_PAIR_PINNED]
+    for _, a, b, sh in batched_items() + serve_units():
+        out += [(k, sh) for k in range(a, b + 1) if will_search(k)]
+    seen, uniq = set(), []
+    for p in out:
+        if p not in seen:
+            seen.add(p)
+            uniq.append(p)
+    return uniq
+
+
 def workload_batched(ctx, A, args, world):
     """Batched persistent form vs plain one-K-per-launch-sequence form on the
     same seeded mixed work items (log-uniform lengths 1..64 K, SHIFT from

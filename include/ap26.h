@@ -5,9 +5,12 @@
  * candidate set (SHIFT, SHIFT+64, ..., SHIFT+576), and reports each one raw,
  * exactly as the reference's GPU kernel checkn (ibethune/ap26,
  * src/opencl/kernels/checkn.cl:198-202) and CPU search
- * (src/cpu/cpuavx2.cpp:548-552) hand it to ReportSolution.  Hashing,
- * 9-base validation and SOL output stay on the host (ap26_report below),
- * byte-compatible with src/common/AP26.cpp.
+ * (src/cpu/cpuavx2.cpp:548-552) hand it to ReportSolution.  ReportSolution
+ * itself (hash, 9-base validation, split recursion, SOL lines;
+ * src/common/AP26.cpp:484-602) runs on the device behind ap26_search_k_sol,
+ * ap26_report_batch and the batched and serving forms; ap26_report below is
+ * the same step on the host for callers that keep their own, byte-compatible
+ * with src/common/AP26.cpp.
  *
  * Conventions: plain pointers and sizes; the caller owns every buffer; every
  * entry point returns an int status (0 = AP26_OK, < 0 = error) and never
@@ -214,7 +217,7 @@ int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *aps,
 /* ---- kernel-level entry points (parity and roofline measurements) -------- */
 /* Sieve only, over n53 starts [q_begin, q_end) of K (0 <= q < 137375320):
  * candidate values n (unordered) into cand[0..cap); *n_cand = total.
- * Replaces the sieve kernel (src/opencl/kernels/sieve.cl:218-362). */
+ * Replaces the sieve kernel (src/opencl/kernels/sieve.cl:12-156). */
 int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin,
                      int64_t q_end, int64_t *cand, int64_t cap,
                      int64_t *n_cand, ap26_stats *stats);
@@ -255,9 +258,13 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  * valid once that stream reaches this point.
  * - Allocates nothing (no cudaMalloc/cudaFree, no context object): all
  *   scratch -- job descriptors, tables, counters -- lives in one
- *   file-scope device array of about 660 KB that every GPU loading the
- *   library keeps until process exit.  At most AP26_NOALLOC_MAX_K values of
- *   K per call; more returns AP26_E_CAPACITY.
+ *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (665,696 bytes)
+ *   that every GPU loading the library keeps until process exit.  At most
+ *   AP26_NOALLOC_MAX_K values of K per call; more returns AP26_E_CAPACITY.
+ *   An invalid K costs no sieve time.
+ * - A CUDA error already pending in the calling thread when the call starts
+ *   is neither returned as this call's own nor cleared: the call launches
+ *   nothing and returns AP26_E_CUDA.
  * - The first call on a device sets that device up synchronously (looks up
  *   the array's device address, fills the constant tables), so it must come
  *   before any stream capture.
@@ -265,6 +272,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  *   calls whose work overlaps on the GPU (other streams, other threads)
  *   race on it and must be serialised by the caller. */
 #define AP26_NOALLOC_MAX_K 64
+#define AP26_NOALLOC_SCRATCH_BYTES 665696
 int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
                              int64_t *d_counts, void *stream);
 

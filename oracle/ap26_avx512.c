@@ -8,7 +8,7 @@
  * candidate each comes from.  Two changes of method, both exact:
  *
  *   sieve  Instead of one OKOK_{p,w} table per prime and shift word
- *          (cpusse2.cpp:38-43, sieve.cl:238-320), bit i of the 640-bit
+ *          (cpusse2.cpp:38-43, sieve.cl:28-113), bit i of the 640-bit
  *          mask of all 10 words is B_p[s + i] with s = n59 * MOD^-1 mod p and
  *          B_p[j] = OK_p[((j + SHIFT) * MOD) mod p], a p-periodic bitstring
  *          (one ~2.5 KB table set per K and SHIFT).  The ten 64-bit window

@@ -14,12 +14,18 @@
 #
 # Flags follow the reference's own makefile (src/cpu/Makefile_linux:10-38) minus
 # BOINC: -O3 -m64, per-file -mavx2 / -mavx / -msse4.1 / -msse2.
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [--if-present] [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $AP26_REFERENCE, else the read-only tree this
+#   recipe was written against (/root/reference).  With --if-present a missing
+#   tree is not an error: the recipe builds nothing and exits 0.
 set -euo pipefail
-REF="${1:-/root/reference}"
+IF_PRESENT=0
+if [ "${1:-}" = "--if-present" ]; then IF_PRESENT=1; shift; fi
+REF="${1:-${AP26_REFERENCE:-/root/reference}}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/common/AP26.cpp" ]; then
+  if [ "$IF_PRESENT" = 1 ]; then exit 0; fi
   echo "reference sources not found under $REF" >&2
   exit 1
 fi

@@ -11,14 +11,21 @@
  *                   hash update or validation, so the record is the
  *                   reference's own candidate->AP output;
  *   PrimeQ          is the reference's own, from src/common/PrimeQ_x86.h
- *                   (included from the reference tree at build time);
+ *                   (included from the reference tree at build time), behind
+ *                   a thin wrapper that counts sieve survivors: every
+ *                   candidate n that passes the reference's sieve and its
+ *                   7..23 / OK_p filters starts exactly one chain walk, whose
+ *                   first call is PrimeQ(n + 5*STEP) (cpuavx2.cpp:532-546);
+ *                   the wrapper tells first calls from the walk's
+ *                   continuations (below) and counts them;
  *   checkpoint      no-op (the CLI's state handling is not under test here);
  *   Progress        counts ticks; in "sample" mode it ends the search early
  *                   with longjmp after a bounded number of ticks, which turns
  *                   the reference's whole-K search into a bounded CPU sample.
  *
  * Modes:
- *   ref_harness raw    K SHIFT [avx2|sse2]   -> "R k K first" lines + summary
+ *   ref_harness raw    K SHIFT [avx2|sse2]   -> "R k K first" lines, then
+ *                      "COUNT survivors" and the summary
  *   ref_harness sample K SHIFT TICKS [avx2|sse2] [ITER]
  *                      -> "SAMPLE K n43_done total_n43_units seconds isa ITER
  *                          setup_seconds tick_seconds"
@@ -43,7 +50,11 @@
 #include <setjmp.h>
 #include <time.h>
 
+/* the reference's PrimeQ under another name; PrimeQ itself is the counting
+ * wrapper defined below */
+#define PrimeQ ref_PrimeQ
 #include "PrimeQ_x86.h"   /* reference: src/common/PrimeQ_x86.h */
+#undef PrimeQ
 
 void Search_avx2(int K, int startSHIFT, int ITER, int K_COUNT, int K_DONE);
 void Search_sse2(int K, int startSHIFT, int ITER, int K_COUNT, int K_DONE);
@@ -63,6 +74,42 @@ void Progress(double prog) {
     g_t_end = now_s();
     longjmp(g_abort, 1);
   }
+}
+
+/* Survivor count from the chain walk's call pattern (cpuavx2.cpp:532-546):
+ *   k=0; m=n+5S; while (PrimeQ(m)) { k++; m+=S; }
+ *   if (k>=10) { m=n+4S; while (m>0 && PrimeQ(m)) { k++; m-=S; } }
+ * After a call that returned true the next call continues the same walk at
+ * m+S (forward) or m-S (backward).  After a forward walk that ended false
+ * with k >= 10 the next call is the backward start n+4S.  Every other call
+ * is the first call of a new candidate.  A backward walk that stops at
+ * m <= 0 makes no call, so a continuation is also checked by its argument. */
+static int64_t g_step = 0;
+static long long g_survivors = 0;
+static int64_t g_last = 0, g_first = 0;
+static int g_last_true = 0, g_fwd = 1, g_fwd_k = 0, g_started = 0;
+
+int PrimeQ(int64_t N) {
+  const int r = ref_PrimeQ(N);
+  int cont = 0;
+  if (g_started && g_last_true) {
+    if (g_fwd && N == g_last + g_step) cont = 1;
+    else if (!g_fwd && N == g_last - g_step) cont = 1;
+  } else if (g_started && g_fwd && g_fwd_k >= 10 && N == g_first - g_step) {
+    g_fwd = 0;                       /* backward start n + 4S */
+    cont = 1;
+  }
+  if (!cont) {
+    g_survivors++;
+    g_started = 1;
+    g_first = N;
+    g_fwd = 1;
+    g_fwd_k = 0;
+  }
+  if (g_fwd && r) g_fwd_k++;
+  g_last = N;
+  g_last_true = r;
+  return r;
 }
 
 void ReportSolution(int AP_Length, int difference, int64_t First_Term) {
@@ -118,6 +165,7 @@ int main(int argc, char **argv) {
   int use_sse2 = !strcmp(isa, "sse2");
   int passes = use_sse2 ? 10 : 3;
 
+  g_step = (int64_t)K * 223092870LL;   /* K * 23#, CONST.H:7 */
   double t0 = now_s();
   if (setjmp(g_abort) == 0) {
     if (use_sse2) Search_sse2(K, SHIFT, iter, 1, 0);
@@ -133,6 +181,7 @@ int main(int argc, char **argv) {
     printf("SAMPLE %d %ld %ld %.6f %s %d %.6f %.6f\n", K, done, 10840L * passes, dt, isa, iter,
            g_t_first - t0, g_t_end - g_t_first);
   } else {
+    printf("COUNT %lld\n", g_survivors);
     printf("DONE %d %ld %.3f %s\n", K, g_reports, dt, isa);
   }
   return 0;

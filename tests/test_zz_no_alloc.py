@@ -8,16 +8,24 @@ the entry point's scratch lives in a fixed device array inside the library.
 
 Checked through the C ABI against the allocating entry point
 (ap26_sieve_count) on two calls in a row, the second with fewer K than the
-first so stale counts from the first call would show.  The counts are
-integers: equality is exact.  This file sorts last so that a stop-at-first-
-failure run has executed every other test before it; it also passes alone in
-a fresh process (the first call sets the device up itself).
+first so stale counts from the first call would show; against survivor
+counts recorded from the reference itself (K=366384 at SHIFT 0 is the
+reference's known answer, src/opencl/AP26.h:343); and with invalid K mixed
+into a call, which must read -1 without disturbing the valid entries or
+costing sieve time.  The counts are integers: equality is exact.  This file
+sorts last so that a stop-at-first-failure run has executed every other test
+before it; it also passes alone in a fresh process (the first call sets the
+device up itself).
 """
 import ctypes
+import json
+import os
+import time
 
 import pytest
 
 import ap26_b200 as A
+from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
@@ -61,3 +69,34 @@ def test_noalloc_rejects_sizes_beyond_its_maximum():
     rc = A.lib.ap26_sieve_count_noalloc(0, ctypes.c_void_p(d_k.data_ptr()), 65, 0,
                                         ctypes.c_void_p(d_out.data_ptr()), None)
     assert rc == A.E_CAPACITY
+
+
+def test_noalloc_counts_equal_reference_survivor_counts():
+    import torch
+    torch.cuda.init()
+    assert _noalloc([366384], 0) == [38838420]
+    pinned = json.load(open(os.path.join(GOLDEN, "shift_counts.json")))
+    by_shift = {}
+    for p in pinned:
+        by_shift.setdefault(p["shift"], []).append(p)
+    for shift, ps in sorted(by_shift.items())[:2]:
+        ps = ps[:2]
+        assert _noalloc([p["K"] for p in ps], shift) == [p["candidates"] for p in ps], shift
+
+
+def test_noalloc_invalid_k_reads_minus_one_and_costs_no_sieve_time():
+    import torch
+    torch.cuda.init()
+    good = 366384
+    t0 = time.perf_counter()
+    one = _noalloc([good], 0)
+    t_one = time.perf_counter() - t0
+    mixed = [0, good, A.KMAX_SAFE + 1, -5]
+    t0 = time.perf_counter()
+    got = _noalloc(mixed, 0)
+    t_mixed = time.perf_counter() - t0
+    assert one == [38838420]
+    assert got == [-1, 38838420, -1, -1]
+    # each invalid K used to cost a whole K of sieving; now only the valid one runs
+    assert t_mixed < 1.5 * t_one + 0.05, (t_mixed, t_one)
+    assert _noalloc([0, -1], 0) == [-1, -1]
