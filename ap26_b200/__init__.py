@@ -38,7 +38,8 @@ class Opts(ctypes.Structure):
                 ("block_threads", ctypes.c_int32), ("late_stage", ctypes.c_int32),
                 ("chunk_tiles", ctypes.c_int32), ("use_graphs", ctypes.c_int32),
                 ("profile", ctypes.c_int32), ("cand_ring_log2", ctypes.c_int32),
-                ("mem_budget", ctypes.c_int64), ("wait_timeout_s", ctypes.c_double)]
+                ("mem_budget", ctypes.c_int64), ("wait_timeout_s", ctypes.c_double),
+                ("tail_group", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class AP(ctypes.Structure):
@@ -104,12 +105,17 @@ def _load():
         "ap26_list_variants": (I, [P, I]),
         "ap26_search_k": (I, [P, I, I, P, I, P, P]),
         "ap26_search_k_sol": (I, [P, I, I, I, P, P, I, P, P]),
+        "ap26_search_k_sol_words": (I, [P, I, I, I, P, P, P, P, I, P, P]),
         "ap26_sprp_bases": (I, [P, P, P, I64, P, P]),
         "ap26_report_batch": (I, [P, P, I64, P, P, P]),
         "ap26_search_batch": (I, [P, P, I, P, I64, P, P, P]),
         "ap26_serve_submit": (I, [P, P]),
+        "ap26_serve_submit_from": (I, [P, P, I, I, ctypes.c_int32]),
         "ap26_serve_step": (I, [P, P]),
+        "ap26_serve_wait": (I, [P, ctypes.c_double]),
         "ap26_serve_poll": (I, [P, P, P, I64, P]),
+        "ap26_serve_checkpoint": (I, [P, I64, P, P, P, P, P, P]),
+        "ap26_serve_memory": (I, [P, P, P]),
         "ap26_sieve_range": (I, [P, I, I, I64, I64, P, I64, P, P]),
         "ap26_sieve_count": (I, [P, P, I, I, P, P]),
         "ap26_sprp_batch": (I, [P, P, I64, P, P]),
@@ -137,8 +143,10 @@ lib = _load()
 # Every symbol include/ap26.h declares (checked by the CPU test suite).
 EXPORTS = ("ap26_version", "ap26_strerror", "ap26_last_error", "ap26_create", "ap26_destroy",
            "ap26_get_opts", "ap26_set_opts", "ap26_list_variants", "ap26_search_k",
-           "ap26_search_k_sol", "ap26_search_batch", "ap26_serve_submit",
-           "ap26_serve_step", "ap26_serve_poll", "ap26_sieve_range", "ap26_sieve_count",
+           "ap26_search_k_sol", "ap26_search_k_sol_words", "ap26_search_batch",
+           "ap26_serve_submit", "ap26_serve_submit_from", "ap26_serve_step", "ap26_serve_wait",
+           "ap26_serve_poll", "ap26_serve_checkpoint", "ap26_serve_memory",
+           "ap26_sieve_range", "ap26_sieve_count",
            "ap26_sprp_batch", "ap26_sprp_bases", "ap26_report_batch", "ap26_chain_batch",
            "ap26_autotune", "ap26_probe_peaks",
            "ap26_sieve_count_noalloc",
@@ -212,7 +220,8 @@ def list_variants():
     arr = (Opts * n)()
     lib.ap26_list_variants(arr, n)
     return [{"dense_primes": o.dense_primes, "warp_queue": o.warp_queue,
-             "block_threads": o.block_threads, "late_stage": o.late_stage} for o in arr]
+             "block_threads": o.block_threads, "late_stage": o.late_stage,
+             "tail_group": o.tail_group} for o in arr]
 
 
 def _aps_to_list(arr, n):
@@ -287,6 +296,22 @@ class Context:
                                           out, cap, ctypes.byref(n), ctypes.byref(st)),
                     "ap26_search_k_sol")
         return h.value, [(out[i].len, out[i].K, out[i].first) for i in range(n.value)], st
+
+    def search_k_sol_words(self, K, shift=0, result_hash=0, iter=0, cap=1 << 12):
+        """search_k_sol with per-word progress: (new result_hash, SOL lines,
+        word of each SOL line, hash after each shift word (10), stats)."""
+        out = (Sol * cap)()
+        words = (ctypes.c_int32 * cap)()
+        at = (ctypes.c_int32 * 10)()
+        h = ctypes.c_int32(result_hash)
+        n = ctypes.c_int(0)
+        st = Stats()
+        self._check(lib.ap26_search_k_sol_words(self.h, int(K), int(shift), int(iter),
+                                                ctypes.byref(h), at, out, words, cap,
+                                                ctypes.byref(n), ctypes.byref(st)),
+                    "ap26_search_k_sol_words")
+        return (h.value, [(out[i].len, out[i].K, out[i].first) for i in range(n.value)],
+                list(words[:n.value]), list(at), st)
 
     def report_batch(self, aps, result_hash=None):
         """Device-side ReportSolution of raw reports [(k, K, first[, n])]:
@@ -378,10 +403,38 @@ class Context:
         it = Item(int(uid), int(kmin), int(kmax), int(shift), 0)
         return lib.ap26_serve_submit(self.h, ctypes.byref(it))
 
+    def serve_submit_from(self, uid, kmin, kmax, shift, K, ITER, result_hash):
+        it = Item(int(uid), int(kmin), int(kmax), int(shift), 0)
+        return lib.ap26_serve_submit_from(self.h, ctypes.byref(it), int(K), int(ITER),
+                                          int(result_hash))
+
     def serve_step(self):
         active = ctypes.c_int(0)
         self._check(lib.ap26_serve_step(self.h, ctypes.byref(active)), "ap26_serve_step")
         return active.value
+
+    def serve_wait(self, max_wait_s):
+        """True once the oldest queued slice has finished (or none is queued)."""
+        rc = lib.ap26_serve_wait(self.h, float(max_wait_s))
+        if rc == E_TIMEOUT:
+            return False
+        self._check(rc, "ap26_serve_wait")
+        return True
+
+    def serve_checkpoint(self, uid):
+        """(kmin, kmax, shift, K, ITER, result_hash) of a unit's device checkpoint."""
+        v = [ctypes.c_int() for _ in range(5)]
+        h = ctypes.c_int32()
+        self._check(lib.ap26_serve_checkpoint(self.h, int(uid), *[ctypes.byref(x) for x in v],
+                                              ctypes.byref(h)), "ap26_serve_checkpoint")
+        return tuple(x.value for x in v) + (h.value,)
+
+    def serve_memory(self):
+        """(bytes held, budget) of the serving pool."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib.ap26_serve_memory(self.h, ctypes.byref(a), ctypes.byref(b)),
+                    "ap26_serve_memory")
+        return a.value, b.value
 
     def serve_poll(self, ap_cap=1 << 16):
         res = ItemResult()

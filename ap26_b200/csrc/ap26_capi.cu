@@ -25,33 +25,18 @@
 namespace ap26 {
 
 // ---- per-job set-up kernel ----------------------------------------------------
-// Thread 0: the reference's per-K constants (src/opencl/AP26.h:112-120, int64
-// split multiplications).  All threads: the bitstrings
-//   B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
-// OK_p[r] = 0 iff r = (jj * (STEP mod p)) mod p for some jj in [p-23, p]
-// (MAKE_OK, src/cpu/cpusse2.cpp:32-36; setok.cl:79-81).
+// The reference's per-K constants (src/opencl/AP26.h:112-120, int64 split
+// multiplications).
 __device__ int kmul_mod(int64_t c, int K, int64_t *out) {
   *out = (c * (K % 17835) + ((c * 17835) % MOD) * (K / 17835)) % MOD;
   return 0;
 }
 
-__global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables) {
-  const int j = blockIdx.x;
-  if (j >= njobs) return;
-  KJob &J = jobs[j];
-  const int K = J.K, shift = J.shift;
-  if (threadIdx.x == 0) {
-    J.STEP = (int64_t)K * PRIM23;
-    J.n0 = (N0 * (K % 17835) + ((N0 * 17835) % MOD) * (K / 17835) + N30) % MOD;
-    kmul_mod(PRES2, K, &J.S31);
-    kmul_mod(PRES3, K, &J.S37);
-    kmul_mod(PRES4, K, &J.S41);
-    kmul_mod(PRES5, K, &J.S43);
-    kmul_mod(PRES6, K, &J.S47);
-    kmul_mod(PRES7, K, &J.S53);
-    kmul_mod(PRES8, K, &J.S59);
-  }
-  uint32_t *tab = tables + (size_t)j * TABLE_WORDS;
+// The sieve bitstrings of one (K, SHIFT), built by all threads of a block:
+//   B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
+// OK_p[r] = 0 iff r = (jj * (STEP mod p)) mod p for some jj in [p-23, p]
+// (MAKE_OK, src/cpu/cpusse2.cpp:32-36; setok.cl:79-81).
+__device__ void build_table(int K, int shift, uint32_t *tab) {
   for (int t = threadIdx.x; t < TABLE_WORDS; t += blockDim.x) {
     int g = 0;
     while (g + 1 < NPRIMES && c_params[g + 1].off <= t) g++;
@@ -77,6 +62,28 @@ __global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables) {
     }
     tab[t] = word;
   }
+}
+
+// Block j: job j.  Thread 0 sets the reference's per-K constants; the block
+// builds the job's bitstrings at KJob::table unless build_tables is 0 (a
+// serving unit builds its tables once, at admission).
+__global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables, int build_tables) {
+  const int j = blockIdx.x;
+  if (j >= njobs) return;
+  KJob &J = jobs[j];
+  const int K = J.K;
+  if (threadIdx.x == 0) {
+    J.STEP = (int64_t)K * PRIM23;
+    J.n0 = (N0 * (K % 17835) + ((N0 * 17835) % MOD) * (K / 17835) + N30) % MOD;
+    kmul_mod(PRES2, K, &J.S31);
+    kmul_mod(PRES3, K, &J.S37);
+    kmul_mod(PRES4, K, &J.S41);
+    kmul_mod(PRES5, K, &J.S43);
+    kmul_mod(PRES6, K, &J.S47);
+    kmul_mod(PRES7, K, &J.S53);
+    kmul_mod(PRES8, K, &J.S59);
+  }
+  if (build_tables) build_table(K, J.shift, tables + (size_t)J.table * TABLE_WORDS);
 }
 
 // Chunk bookkeeping; `ring` selects the candidate ring this chunk fills.
@@ -229,6 +236,9 @@ static const SieveVariant kVariants[] = {
     AP26_VARIANT(20, 4, 44, 384, 128, 8),
     AP26_VARIANT(24, 4, 52, 320, 96, 12),
     AP26_VARIANT(20, 4, 44, 320, 96, 4),
+    AP26_VARIANT(20, 6, 48, 320, 96, 8),
+    AP26_VARIANT(18, 6, 44, 320, 96, 8),
+    AP26_VARIANT(22, 4, 52, 320, 96, 8),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -237,40 +247,136 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 using namespace ap26;
 
 // ---- context --------------------------------------------------------------------
-// A serving unit's running state, kept on the device in the unit's slot:
-// the partial ReportSolution hash sum, survivor count and K-jobs finished.
+// A serving unit's state, kept on the device in the unit's slot: the running
+// ReportSolution hash sum, survivor count and K-jobs finished, and the unit's
+// checkpoint in the fields of the reference's state file (write_state,
+// src/common/AP26.cpp:360-390): every K below K_next is searched, K_next from
+// shift word iter on, and result_hash is the reference's result_hash there.
 struct UnitState {
-  unsigned long long hash_add;
+  unsigned long long hash_add;   // sum of first%1000 + len over the unit's reports so far
   unsigned long long candidates;
   int32_t ks_done;
-  int32_t pad;
+  int32_t K_next;
+  int32_t iter;
+  int32_t result_hash;           // fold(h0, hash_add)
+  int32_t h0;                    // result_hash the unit started from
+  int32_t kmin, kmax, shift;
 };
 constexpr int kUnitSlots = 1024;
 
-// After a serving slice: each K-job's survivor count and ReportSolution hash
-// sum go into its unit's slot (KJob::item holds the slot).
+constexpr long long kMaxIntV = 2000000000;   // MAXINTV, AP26.cpp:88
+
+// result_hash after adding `add` through ReportSolution calls, each of which
+// adds first%1000 + len and subtracts MAXINTV when above it (AP26.cpp:556-560):
+// for a start in [0, MAXINTV] the value stays in [0, MAXINTV], is congruent
+// to the total and is 0 only for a zero total.
+__host__ __device__ inline int32_t hash_fold(int32_t h0, unsigned long long add) {
+  const unsigned long long total = (unsigned long long)h0 + add;
+  if (total == 0) return 0;
+  return (int32_t)((total - 1) % (unsigned long long)kMaxIntV + 1);
+}
+
+// After a serving slice (one block): each K-job's survivor count and
+// ReportSolution hash sums go into its unit's slot (KJob::item holds the
+// slot), then every touched slot's checkpoint advances past its finished K.
+// A unit's K-jobs run in ascending K and a slice finishes all of its jobs,
+// so the checkpoint K is the largest finished K + 1.
 __global__ void unit_accumulate_kernel(const KJob *jobs, int njobs,
                                        const unsigned long long *job_counts,
-                                       const unsigned long long *job_hash, UnitState *units) {
+                                       const unsigned long long *job_hash, UnitState *units,
+                                       UnitState *snap) {
   for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
     UnitState &u = units[jobs[j].item];
-    atomicAdd(&u.hash_add, job_hash[j]);
+    unsigned long long h = 0;
+    for (int w = 0; w < WORDS; w++) h += job_hash[j * WORDS + w];
+    atomicAdd(&u.hash_add, h);
     atomicAdd(&u.candidates, job_counts[j]);
     atomicAdd(&u.ks_done, 1);
+    atomicMax(&u.K_next, jobs[j].K + 1);
   }
+  __syncthreads();
+  for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
+    UnitState &u = units[jobs[j].item];
+    u.iter = 0;
+    u.result_hash = hash_fold(u.h0, u.hash_add);
+  }
+  __syncthreads();
+  // the slice's copy of each of its units' state, read back in stream order
+  for (int j = threadIdx.x; j < njobs; j += blockDim.x) snap[j] = units[jobs[j].item];
 }
+
+// Admission of a serving unit: its slot's initial state (first launch only)
+// and the sieve bitstrings of up to kAdmitMax of its K, one block per K,
+// into the serving pool.  Everything travels as kernel parameters, so
+// admission needs no staging buffer and no wait on work already queued.
+constexpr int kAdmitMax = 448;
+struct AdmitArgs {
+  UnitState init;
+  int32_t slot, write_init, shift, n;
+  int32_t K[kAdmitMax];
+  int32_t table[kAdmitMax];
+};
+static_assert(sizeof(AdmitArgs) <= 4000, "kernel parameters stay below 4 KB");
+
+__global__ void admit_unit_kernel(const AdmitArgs a, UnitState *units, uint32_t *pool) {
+  if (a.write_init && blockIdx.x == 0 && threadIdx.x == 0) units[a.slot] = a.init;
+  if ((int)blockIdx.x < a.n)
+    build_table(a.K[blockIdx.x], a.shift, pool + (size_t)a.table[blockIdx.x] * TABLE_WORDS);
+}
+
+// Device and pinned host buffers of one pipeline run: K-job descriptors and
+// (unless a serving pool provides them) their tables, per-job counters and
+// per-word hash sums, run state, raw reports and ReportSolution results.
+struct JobSet {
+  int cap = 0;                        // K-jobs
+  long long ap_cap = 0;               // raw reports
+  bool own_tables = true;             // tables here, job j's at index j
+  KJob *d_jobs = nullptr, *h_jobs = nullptr;
+  uint32_t *d_tables = nullptr;
+  unsigned long long *d_job_counts = nullptr, *h_job_counts = nullptr;
+  unsigned long long *d_job_hash = nullptr, *h_job_hash = nullptr;   // cap * WORDS
+  DevState *d_st = nullptr, *h_st = nullptr;
+  APRec *d_aps = nullptr, *h_aps = nullptr;
+  FinRec *d_fin = nullptr, *h_fin = nullptr;
+  cudaEvent_t t0 = nullptr, done = nullptr;   // around the run, on the main stream
+  // shape of the run last enqueued into this set
+  int njobs = 0;
+  bool count_only = false;
+  unsigned long long nchunks = 0, nprof = 0;
+  int launches = 0;
+};
+
+// A cached CUDA graph of one whole run shape.
+struct GraphEntry {
+  long long key[7];
+  cudaGraphExec_t exec;
+  unsigned long long used;
+};
+constexpr size_t kMaxGraphs = 8;
 
 struct ServeUnit {
   ap26_item item;
-  std::vector<int> ks;           // searchable K of the unit
+  std::vector<int> ks;           // searchable K of the unit still to search
+  std::vector<int> tables;       // its tables in the serving pool, one per K of ks
+  int iter0 = 0;                 // first shift word of ks[0] (a resumed unit)
   size_t next_k = 0;             // next K to put on the device
-  int inflight = 0;              // K-jobs of this unit in the current slice
   int done_k = 0;                // host copy of the count, for scheduling
   int slot = -1;                 // its UnitState on the device
   std::vector<ap26_ap> aps;
   int status = AP26_OK;
   std::chrono::steady_clock::time_point t_submit;
   double latency_ms = 0;
+  int64_t bytes = 0;             // device bytes it holds while admitted
+  UnitState snap;                // its slot as of its last finished slice
+};
+
+// A serving slice in flight: its job set and, per job, the unit it serves.
+struct Slice {
+  JobSet set;
+  std::vector<int64_t> unit_ids;   // per job
+  UnitState *d_snap = nullptr, *h_snap = nullptr;   // per job: its unit's state after it
+  bool busy = false;
+  int rc = AP26_OK;
 };
 
 struct ap26_ctx {
@@ -279,36 +385,28 @@ struct ap26_ctx {
   int variant = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;              // chain walks of the overlapped form
+  cudaStream_t copy_stream = nullptr;          // read-backs of finished serving slices
   cudaEvent_t sieve_done[2] = {nullptr, nullptr}, chain_done[2] = {nullptr, nullptr};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 0, sieve_blocks = 0, chain_blocks = 0;
-  // device buffers
-  KJob *d_jobs = nullptr;
-  uint32_t *d_tables = nullptr;
-  unsigned long long *d_job_counts = nullptr;
-  int jobs_cap = 0;
-  DevState *d_st = nullptr;
-  Cand *d_cand[2] = {nullptr, nullptr};   // two candidate rings (overlapped form)
+  JobSet main;                                 // every synchronous entry point
+  Cand *d_cand[2] = {nullptr, nullptr};        // two candidate rings (overlapped form)
   long long cand_cap = 0;
-  APRec *d_aps = nullptr;
-  long long ap_cap = 0;
-  FinRec *d_fin = nullptr;                   // ReportSolution result per report
-  unsigned long long *d_job_hash = nullptr;  // per-job sum of hash contributions
-  // pinned host mirrors
-  KJob *h_jobs = nullptr;
-  DevState *h_st = nullptr;
-  APRec *h_aps = nullptr;
-  FinRec *h_fin = nullptr;
-  unsigned long long *h_job_counts = nullptr, *h_job_hash = nullptr;
   // graphs
-  cudaGraphExec_t chunk_graph = nullptr;
-  long long graph_key = -1;
-  std::vector<cudaEvent_t> prof_events;   // per-sieve-launch timing pairs
+  std::vector<GraphEntry> graphs;
+  unsigned long long graph_clock = 0;
+  std::vector<cudaEvent_t> prof_events;        // per-sieve-launch timing pairs
   // serving
   std::deque<ServeUnit> units;
   std::deque<ServeUnit> finished;
-  int64_t bytes_in_use = 0;     // device bytes held by admitted serving units
-  UnitState *d_units = nullptr; // kUnitSlots serving-unit states
+  Slice slices[2];
+  std::deque<int> inflight;                    // slice indices, oldest first
+  uint32_t *d_pool = nullptr;                  // serving units' tables
+  int pool_tables = 0;
+  std::vector<int> free_tables;
+  int64_t bytes_in_use = 0;                    // device bytes held by admitted units
+  int64_t serve_budget = 0;                    // pool + fixed serving buffers
+  UnitState *d_units = nullptr;                // kUnitSlots serving-unit states
   std::vector<int> free_slots;
   std::string last_error;
   bool pending = false;        // a call timed out with its work still queued
@@ -350,7 +448,7 @@ struct DevBuf {
   cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * n); }
 };
 
-extern "C" int ap26_version(void) { return 10000; }
+extern "C" int ap26_version(void) { return 10100; }
 
 extern "C" const char *ap26_strerror(int code) {
   switch (code) {
@@ -377,9 +475,10 @@ static int default_opts(ap26_opts *o) {
   if (!o->warp_queue) o->warp_queue = kVariants[0].QCAP;
   if (!o->block_threads) o->block_threads = kVariants[0].WARPS * 32;
   if (!o->late_stage) o->late_stage = kVariants[0].SL;
-  if (!o->chunk_tiles) o->chunk_tiles = 32768;
-  if (!o->mem_budget) o->mem_budget = (int64_t)8 << 30;
-  if (!o->cand_ring_log2) o->cand_ring_log2 = 23;
+  if (!o->tail_group) o->tail_group = kVariants[0].R;
+  if (!o->chunk_tiles) o->chunk_tiles = 131072;
+  if (!o->use_graphs) o->use_graphs = 1;
+  if (!o->cand_ring_log2) o->cand_ring_log2 = 25;
   if (!(o->wait_timeout_s > 0)) o->wait_timeout_s = 3600.0;
   return 0;
 }
@@ -388,10 +487,15 @@ static int pick_variant(const ap26_opts &o) {
   for (int i = 0; i < kNumVariants; i++) {
     const SieveVariant &v = kVariants[i];
     if (v.G == o.dense_primes && v.QCAP == o.warp_queue && v.WARPS * 32 == o.block_threads &&
-        v.SL == o.late_stage)
+        v.SL == o.late_stage && v.R == o.tail_group)
       return i;
   }
   return -1;
+}
+
+static void drop_graphs(ap26_ctx *ctx) {
+  for (auto &g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+  ctx->graphs.clear();
 }
 
 static int set_variant(ap26_ctx *ctx, int vi) {
@@ -406,42 +510,66 @@ static int set_variant(ap26_ctx *ctx, int vi) {
   ctx->opts.warp_queue = v.QCAP;
   ctx->opts.block_threads = v.WARPS * 32;
   ctx->opts.late_stage = v.SL;
-  if (ctx->chunk_graph) {
-    cudaGraphExecDestroy(ctx->chunk_graph);
-    ctx->chunk_graph = nullptr;
-  }
+  ctx->opts.tail_group = v.R;
+  drop_graphs(ctx);
   return AP26_OK;
 }
 
-static int ensure_jobs(ap26_ctx *ctx, int njobs) {
-  if (njobs <= ctx->jobs_cap) return AP26_OK;
-  int cap = std::max(njobs, std::max(64, ctx->jobs_cap * 2));
-  const int64_t need = (int64_t)cap * (sizeof(KJob) + TABLE_WORDS * 4 + 8);
-  if (cap > 64 && need > ctx->opts.mem_budget) return AP26_E_NOMEM;
-  if (ctx->d_jobs) {
+static void jobset_free(JobSet &S) {
+  cudaFree(S.d_jobs); cudaFree(S.d_tables); cudaFree(S.d_job_counts); cudaFree(S.d_job_hash);
+  cudaFree(S.d_st); cudaFree(S.d_aps); cudaFree(S.d_fin);
+  cudaFreeHost(S.h_jobs); cudaFreeHost(S.h_job_counts); cudaFreeHost(S.h_job_hash);
+  cudaFreeHost(S.h_st); cudaFreeHost(S.h_aps); cudaFreeHost(S.h_fin);
+  if (S.t0) cudaEventDestroy(S.t0);
+  if (S.done) cudaEventDestroy(S.done);
+  const long long ap_cap = S.ap_cap;
+  const bool own = S.own_tables;
+  S = JobSet();
+  S.ap_cap = ap_cap;
+  S.own_tables = own;
+}
+
+// Grows a job set to hold njobs K-jobs (its report capacity is fixed at the
+// first allocation).  Cleared first: a failed allocation leaves no freed
+// pointers behind for jobset_free to free again.
+static int jobset_ensure(ap26_ctx *ctx, JobSet &S, int njobs) {
+  if (njobs <= S.cap && S.d_st) return AP26_OK;
+  const int cap = std::max(njobs, std::max(64, S.cap * 2));
+  if (S.d_st) {
     drain(ctx);
-    cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
-    cudaFree(ctx->d_job_hash);
-    cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts); cudaFreeHost(ctx->h_job_hash);
-    // cleared first: a failed allocation below must not leave freed pointers
-    // for ap26_destroy to free again
-    ctx->d_jobs = nullptr; ctx->d_tables = nullptr; ctx->d_job_counts = nullptr;
-    ctx->d_job_hash = nullptr;
-    ctx->h_jobs = nullptr; ctx->h_job_counts = nullptr; ctx->h_job_hash = nullptr;
-    ctx->jobs_cap = 0;
+    CK(cudaStreamSynchronize(ctx->stream));
+    jobset_free(S);
+    drop_graphs(ctx);   // graphs hold the old buffers' addresses
   }
-  CK(cudaMalloc(&ctx->d_jobs, sizeof(KJob) * cap));
-  CK(cudaMalloc(&ctx->d_tables, sizeof(uint32_t) * TABLE_WORDS * (size_t)cap));
-  CK(cudaMalloc(&ctx->d_job_counts, sizeof(unsigned long long) * cap));
-  CK(cudaMalloc(&ctx->d_job_hash, sizeof(unsigned long long) * cap));
-  CK(cudaMallocHost(&ctx->h_jobs, sizeof(KJob) * cap));
-  CK(cudaMallocHost(&ctx->h_job_counts, sizeof(unsigned long long) * cap));
-  CK(cudaMallocHost(&ctx->h_job_hash, sizeof(unsigned long long) * cap));
-  ctx->jobs_cap = cap;
-  if (ctx->chunk_graph) {
-    cudaGraphExecDestroy(ctx->chunk_graph);
-    ctx->chunk_graph = nullptr;
-  }
+  CK(cudaMalloc(&S.d_jobs, sizeof(KJob) * cap));
+  if (S.own_tables) CK(cudaMalloc(&S.d_tables, sizeof(uint32_t) * TABLE_WORDS * (size_t)cap));
+  CK(cudaMalloc(&S.d_job_counts, sizeof(unsigned long long) * cap));
+  CK(cudaMalloc(&S.d_job_hash, sizeof(unsigned long long) * WORDS * cap));
+  CK(cudaMalloc(&S.d_st, sizeof(DevState)));
+  CK(cudaMalloc(&S.d_aps, sizeof(APRec) * S.ap_cap));
+  CK(cudaMalloc(&S.d_fin, sizeof(FinRec) * S.ap_cap));
+  CK(cudaMallocHost(&S.h_jobs, sizeof(KJob) * cap));
+  CK(cudaMallocHost(&S.h_job_counts, sizeof(unsigned long long) * cap));
+  CK(cudaMallocHost(&S.h_job_hash, sizeof(unsigned long long) * WORDS * cap));
+  CK(cudaMallocHost(&S.h_st, sizeof(DevState)));
+  CK(cudaMallocHost(&S.h_aps, sizeof(APRec) * S.ap_cap));
+  CK(cudaMallocHost(&S.h_fin, sizeof(FinRec) * S.ap_cap));
+  CK(cudaEventCreate(&S.t0));
+  CK(cudaEventCreate(&S.done));
+  S.cap = cap;
+  return AP26_OK;
+}
+
+static unsigned long long job_hash_total(const JobSet &S, int j) {
+  unsigned long long h = 0;
+  for (int w = 0; w < WORDS; w++) h += S.h_job_hash[(size_t)j * WORDS + w];
+  return h;
+}
+
+static int alloc_rings(ap26_ctx *ctx, int log2) {
+  ctx->cand_cap = 1ll << log2;
+  CK(cudaMalloc(&ctx->d_cand[0], sizeof(Cand) * ctx->cand_cap));
+  CK(cudaMalloc(&ctx->d_cand[1], sizeof(Cand) * ctx->cand_cap));
   return AP26_OK;
 }
 
@@ -455,6 +583,7 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
   ctx->device = device;
   if (opts) ctx->opts = *opts;
   default_opts(&ctx->opts);
+  ctx->main.ap_cap = 1ll << 20;
   int rc;
 #define CKC(call)                                     \
   do {                                                \
@@ -470,8 +599,14 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     // 8 x 128 (1126.5 ms against 1130.1 ms); 4 x 128 was slower
     ctx->chain_blocks = prop.multiProcessorCount * 16;
     CKC(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CKC(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+    CKC(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     CKC(cudaEventCreate(&ctx->ev0));
     CKC(cudaEventCreate(&ctx->ev1));
+    for (int r = 0; r < 2; r++) {
+      CKC(cudaEventCreateWithFlags(&ctx->sieve_done[r], cudaEventDisableTiming));
+      CKC(cudaEventCreateWithFlags(&ctx->chain_done[r], cudaEventDisableTiming));
+    }
     // constant tables
     uint16_t trip[NUM_TRIPLES];
     int nt = ap26h_triples(trip);
@@ -481,28 +616,18 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     for (int g = 0; g < NPRIMES; g++) params[g] = make_param(g);
     CKC(cudaMemcpyToSymbol(c_params, params, sizeof(params)));
     // buffers
-    if (ctx->opts.cand_ring_log2 < 12 || ctx->opts.cand_ring_log2 > 26) {
+    if (ctx->opts.cand_ring_log2 < 12 || ctx->opts.cand_ring_log2 > 27) {
       rc = AP26_E_ARG;
       goto fail;
     }
-    ctx->cand_cap = 1ll << ctx->opts.cand_ring_log2;
-    ctx->ap_cap = 1ll << 20;
-    CKC(cudaMalloc(&ctx->d_st, sizeof(DevState)));
-    CKC(cudaMalloc(&ctx->d_cand[0], sizeof(Cand) * ctx->cand_cap));
-    CKC(cudaMalloc(&ctx->d_cand[1], sizeof(Cand) * ctx->cand_cap));
-    CKC(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
-    for (int r = 0; r < 2; r++) {
-      CKC(cudaEventCreateWithFlags(&ctx->sieve_done[r], cudaEventDisableTiming));
-      CKC(cudaEventCreateWithFlags(&ctx->chain_done[r], cudaEventDisableTiming));
-    }
-    CKC(cudaMalloc(&ctx->d_aps, sizeof(APRec) * ctx->ap_cap));
+    if ((rc = alloc_rings(ctx, ctx->opts.cand_ring_log2)) != AP26_OK) goto fail;
     CKC(cudaMalloc(&ctx->d_units, sizeof(UnitState) * kUnitSlots));
     for (int i = kUnitSlots - 1; i >= 0; i--) ctx->free_slots.push_back(i);
-    CKC(cudaMalloc(&ctx->d_fin, sizeof(FinRec) * ctx->ap_cap));
-    CKC(cudaMallocHost(&ctx->h_fin, sizeof(FinRec) * ctx->ap_cap));
-    CKC(cudaMallocHost(&ctx->h_st, sizeof(DevState)));
-    CKC(cudaMallocHost(&ctx->h_aps, sizeof(APRec) * ctx->ap_cap));
-    if ((rc = ensure_jobs(ctx, 64)) != AP26_OK) goto fail;
+    for (int i = 0; i < 2; i++) {
+      ctx->slices[i].set.ap_cap = 1ll << 16;
+      ctx->slices[i].set.own_tables = false;
+    }
+    if ((rc = jobset_ensure(ctx, ctx->main, 64)) != AP26_OK) goto fail;
     int vi = pick_variant(ctx->opts);
     if (vi < 0) { rc = AP26_E_ARG; goto fail; }
     if ((rc = set_variant(ctx, vi)) != AP26_OK) goto fail;
@@ -520,21 +645,26 @@ extern "C" void ap26_destroy(ap26_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
-  if (ctx->chunk_graph) cudaGraphExecDestroy(ctx->chunk_graph);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  drop_graphs(ctx);
   for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
-  cudaFree(ctx->d_jobs); cudaFree(ctx->d_tables); cudaFree(ctx->d_job_counts);
-  cudaFree(ctx->d_job_hash); cudaFree(ctx->d_fin); cudaFree(ctx->d_units);
-  cudaFreeHost(ctx->h_job_hash); cudaFreeHost(ctx->h_fin);
-  cudaFree(ctx->d_st); cudaFree(ctx->d_cand[0]); cudaFree(ctx->d_cand[1]); cudaFree(ctx->d_aps);
+  jobset_free(ctx->main);
+  for (int i = 0; i < 2; i++) {
+    jobset_free(ctx->slices[i].set);
+    cudaFree(ctx->slices[i].d_snap);
+    cudaFreeHost(ctx->slices[i].h_snap);
+  }
+  cudaFree(ctx->d_units);
+  cudaFree(ctx->d_pool);
+  cudaFree(ctx->d_cand[0]); cudaFree(ctx->d_cand[1]);
   for (int r = 0; r < 2; r++) {
     if (ctx->sieve_done[r]) cudaEventDestroy(ctx->sieve_done[r]);
     if (ctx->chain_done[r]) cudaEventDestroy(ctx->chain_done[r]);
   }
-  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
-  cudaFreeHost(ctx->h_jobs); cudaFreeHost(ctx->h_job_counts);
-  cudaFreeHost(ctx->h_st); cudaFreeHost(ctx->h_aps);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -546,9 +676,12 @@ extern "C" int ap26_list_variants(ap26_opts *out, int cap) {
     out[i].warp_queue = kVariants[i].QCAP;
     out[i].block_threads = kVariants[i].WARPS * 32;
     out[i].late_stage = kVariants[i].SL;
+    out[i].tail_group = kVariants[i].R;
   }
   return kNumVariants;
 }
+
+static bool serving_idle(const ap26_ctx *ctx) { return ctx->inflight.empty(); }
 
 extern "C" int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts) {
   if (!ctx || !opts) return AP26_E_ARG;
@@ -557,29 +690,33 @@ extern "C" int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts) {
   if (opts->warp_queue) o.warp_queue = opts->warp_queue;
   if (opts->block_threads) o.block_threads = opts->block_threads;
   if (opts->late_stage) o.late_stage = opts->late_stage;
+  if (opts->tail_group) o.tail_group = opts->tail_group;
   if (opts->chunk_tiles) o.chunk_tiles = opts->chunk_tiles;
   if (opts->mem_budget) o.mem_budget = opts->mem_budget;
   if (opts->cand_ring_log2) o.cand_ring_log2 = opts->cand_ring_log2;
   if (opts->wait_timeout_s > 0) o.wait_timeout_s = opts->wait_timeout_s;
-  o.use_graphs = opts->use_graphs;
+  if (opts->use_graphs) o.use_graphs = opts->use_graphs;
   o.profile = opts->profile;
   const int vi = pick_variant(o);
-  if (vi < 0 || o.cand_ring_log2 < 12 || o.cand_ring_log2 > 26) return AP26_E_ARG;
+  if (vi < 0 || o.cand_ring_log2 < 12 || o.cand_ring_log2 > 27 || o.chunk_tiles < 1)
+    return AP26_E_ARG;
+  if (o.mem_budget != ctx->opts.mem_budget && ctx->d_pool) return AP26_E_ARG;
+  if (!serving_idle(ctx)) return AP26_E_ARG;   // slices in flight use the rings
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
   if (o.cand_ring_log2 != ctx->opts.cand_ring_log2) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream2));
     cudaFree(ctx->d_cand[0]);
     cudaFree(ctx->d_cand[1]);
     ctx->d_cand[0] = ctx->d_cand[1] = nullptr;
-    ctx->cand_cap = 1ll << o.cand_ring_log2;
-    CK(cudaMalloc(&ctx->d_cand[0], sizeof(Cand) * ctx->cand_cap));
-    CK(cudaMalloc(&ctx->d_cand[1], sizeof(Cand) * ctx->cand_cap));
+    drop_graphs(ctx);
+    int rc = alloc_rings(ctx, o.cand_ring_log2);
+    if (rc != AP26_OK) return rc;
   }
-  const int64_t keep_budget = o.mem_budget;
   ctx->opts = o;
   int rc = set_variant(ctx, vi);
-  ctx->opts.mem_budget = keep_budget;
-  if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
+  drop_graphs(ctx);
   return rc;
 }
 
@@ -593,9 +730,8 @@ static bool k_in_domain(int K, int shift) {
   return K >= 1 && K <= AP26_KMAX_SAFE && shift >= 0 && shift <= AP26_SHIFT_MAX;
 }
 
-// Bounded host wait on the stream: polls an event, gives up after timeout_s.
-static int wait_stream(ap26_ctx *ctx, double timeout_s) {
-  cudaEvent_t e = ctx->ev1;
+// Bounded host wait on an event: polls it, gives up after timeout_s.
+static int wait_event(ap26_ctx *ctx, cudaEvent_t e, double timeout_s) {
   auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     cudaError_t q = cudaEventQuery(e);
@@ -611,181 +747,235 @@ static int wait_stream(ap26_ctx *ctx, double timeout_s) {
   }
 }
 
-// Enqueues the chunked pipeline for ctx->h_jobs[0..njobs) (K, shift, q range
-// and item filled by the caller).  count_only: survivors are counted, no
-// chain walk.  Returns after the D2H of state, counts and reports.
-static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
-                    long long *n_aps_out, bool overlap = false) {
+static int ensure_prof_events(ap26_ctx *ctx, unsigned long long n) {
+  while ((unsigned long long)ctx->prof_events.size() < 2 * n) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    ctx->prof_events.push_back(e);
+  }
+  return AP26_OK;
+}
+
+// The whole run of S.h_jobs[0..njobs): H2D of the jobs and the run state,
+// set-up, per chunk of chunk_tiles tiles chunk_begin -> sieve -> chain ->
+// chunk_end (the chain walk of chunk c on the second stream while chunk c+1
+// is sieved into the other candidate ring, when overlapped), ReportSolution
+// of every raw report, and the read-back of the run state, per-job counts and
+// per-word hash sums into the pinned mirrors.  Issued on ctx->stream (and
+// stream2); with `capture` the profiling events become event-record nodes of
+// the graph being captured.
+static cudaError_t emit_run(ap26_ctx *ctx, JobSet &S, const uint32_t *tables, int build_tables,
+                            bool two_streams, bool capture) {
+  cudaStream_t s = ctx->stream;
+  const SieveVariant &V = kVariants[ctx->variant];
+  const int njobs = S.njobs;
+  cudaError_t e;
+#define EM(call) do { if ((e = (call)) != cudaSuccess) return e; } while (0)
+  EM(cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(KJob) * njobs, cudaMemcpyHostToDevice, s));
+  EM(cudaMemcpyAsync(S.d_st, S.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+  EM(cudaMemsetAsync(S.d_job_counts, 0, sizeof(unsigned long long) * njobs, s));
+  EM(cudaMemsetAsync(S.d_job_hash, 0, sizeof(unsigned long long) * WORDS * njobs, s));
+  setup_jobs_kernel<<<njobs, 256, 0, s>>>(S.d_jobs, njobs, const_cast<uint32_t *>(tables),
+                                          build_tables);
+  EM(cudaGetLastError());
+  // ring r: candidate buffer d_cand[r] and its fill count DevState::cand_count[r]
+  SieveArgs sa[2];
+  ChainArgs ca[2];
+  for (int r = 0; r < 2; r++) {
+    sa[r] = sieve_args(S.d_jobs, njobs, tables, S.d_st, ctx->d_cand[r], ctx->cand_cap,
+                       S.d_job_counts, S.count_only ? 1 : 0, &S.d_st->cand_count[r]);
+    ca[r] = chain_args(S.d_jobs, S.d_st, ctx->d_cand[r], ctx->cand_cap, S.d_aps, S.ap_cap,
+                       &S.d_st->cand_count[r]);
+  }
+  const unsigned flag = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+  for (unsigned long long c = 0; c < S.nchunks; c++) {
+    const int r = two_streams ? (int)(c & 1) : 0;
+    // ring r is free once the chain walk of chunk c-2 has read it
+    if (two_streams && c >= 2) EM(cudaStreamWaitEvent(s, ctx->chain_done[r], 0));
+    chunk_begin_kernel<<<1, 1, 0, s>>>(S.d_st, r);
+    if (c < S.nprof) EM(cudaEventRecordWithFlags(ctx->prof_events[2 * c], s, flag));
+    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa[r]);
+    if (c < S.nprof) EM(cudaEventRecordWithFlags(ctx->prof_events[2 * c + 1], s, flag));
+    if (two_streams) {
+      chunk_end_kernel<<<1, 1, 0, s>>>(S.d_st, ctx->cand_cap, r);
+      EM(cudaEventRecord(ctx->sieve_done[r], s));
+      EM(cudaStreamWaitEvent(ctx->stream2, ctx->sieve_done[r], 0));
+      chain_kernel<<<ctx->chain_blocks, kChainThreads, 0, ctx->stream2>>>(ca[r]);
+      EM(cudaEventRecord(ctx->chain_done[r], ctx->stream2));
+    } else {
+      if (!S.count_only) chain_kernel<<<ctx->chain_blocks, kChainThreads, 0, s>>>(ca[r]);
+      chunk_end_kernel<<<1, 1, 0, s>>>(S.d_st, ctx->cand_cap, r);
+    }
+    EM(cudaGetLastError());
+  }
+  if (two_streams) {   // the last chain walks finish before the reports are read
+    EM(cudaStreamWaitEvent(s, ctx->chain_done[0], 0));
+    if (S.nchunks > 1) EM(cudaStreamWaitEvent(s, ctx->chain_done[1], 0));
+  }
+  if (!S.count_only) {
+    // ReportSolution of every report on the device (AP26.cpp:549-602)
+    ReportArgs ra;
+    ra.aps = S.d_aps;
+    ra.count = &S.d_st->ap_count;
+    ra.n = S.ap_cap;
+    ra.jobs = S.d_jobs;
+    ra.fin = S.d_fin;
+    ra.job_hash = S.d_job_hash;
+    report_kernel<<<ctx->num_sms * 2, REPORT_WARPS * 32, 0, s>>>(ra);
+    EM(cudaGetLastError());
+  }
+  EM(cudaMemcpyAsync(S.h_st, S.d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  EM(cudaMemcpyAsync(S.h_job_counts, S.d_job_counts, sizeof(unsigned long long) * njobs,
+                     cudaMemcpyDeviceToHost, s));
+  if (!S.count_only)
+    EM(cudaMemcpyAsync(S.h_job_hash, S.d_job_hash, sizeof(unsigned long long) * WORDS * njobs,
+                       cudaMemcpyDeviceToHost, s));
+#undef EM
+  return cudaSuccess;
+}
+
+// Captures emit_run into a graph (on failure the stream leaves capture mode
+// and the caller runs the work directly).
+static cudaError_t capture_run(ap26_ctx *ctx, JobSet &S, const uint32_t *tables,
+                               int build_tables, bool two_streams, cudaGraphExec_t *exec) {
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t em = emit_run(ctx, S, tables, build_tables, two_streams, true);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(ctx->stream, &g);
+  if (em != cudaSuccess) e = em;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();   // a failed capture leaves no error behind for later calls
+  return e;
+}
+
+// Enqueues the run of S.h_jobs[0..njobs) and returns without waiting:
+// S.done fires once the run state, counts and hash sums are in the pinned
+// mirrors.  With opts.use_graphs the run is one CUDA-graph launch, captured
+// once per run shape and replayed from the cache.
+static int enqueue_jobs(ap26_ctx *ctx, JobSet &S, int njobs, bool count_only, bool overlap,
+                        const uint32_t *tables = nullptr, int build_tables = 1,
+                        bool record_done = true) {
   int rc;
-  drain(ctx);
-  if ((rc = ensure_jobs(ctx, njobs)) != AP26_OK) return rc;
+  if ((rc = jobset_ensure(ctx, S, njobs)) != AP26_OK) return rc;
+  if (!tables) tables = S.d_tables;
   // tile prefix; a tile is one start per thread of the variant's CTA
   const SieveVariant &V = kVariants[ctx->variant];
   const int64_t tile_n53 = (int64_t)V.WARPS * 32;
   unsigned long long tiles = 0;
   for (int j = 0; j < njobs; j++) {
-    KJob &J = ctx->h_jobs[j];
+    KJob &J = S.h_jobs[j];
     const int64_t span = J.q_end - J.q_begin;
     J.ntiles = (int32_t)((span + tile_n53 - 1) / tile_n53);
     J.tile_begin = (int64_t)tiles;
+    if (S.own_tables) J.table = j;
     tiles += (unsigned long long)J.ntiles;
   }
-  memset(ctx->h_st, 0, sizeof(DevState));
-  ctx->h_st->chunk_size = (unsigned long long)ctx->opts.chunk_tiles;
-  ctx->h_st->total_tiles = tiles;
-  cudaStream_t s = ctx->stream;
-  CK(cudaEventRecord(ctx->ev0, s));
-  CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob) * njobs, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(ctx->d_job_counts, 0, sizeof(unsigned long long) * njobs, s));
-  CK(cudaMemsetAsync(ctx->d_job_hash, 0, sizeof(unsigned long long) * njobs, s));
-  setup_jobs_kernel<<<njobs, 256, 0, s>>>(ctx->d_jobs, njobs, ctx->d_tables);
-  CK(cudaGetLastError());
-  int launches = 1;
-  // ring r: candidate buffer d_cand[r] and its fill count DevState::cand_count[r]
-  SieveArgs sa[2];
-  ChainArgs ca[2];
-  for (int r = 0; r < 2; r++) {
-    sa[r] = sieve_args(ctx->d_jobs, njobs, ctx->d_tables, ctx->d_st, ctx->d_cand[r],
-                       ctx->cand_cap, ctx->d_job_counts, count_only ? 1 : 0,
-                       &ctx->d_st->cand_count[r]);
-    ca[r] = chain_args(ctx->d_jobs, ctx->d_st, ctx->d_cand[r], ctx->cand_cap, ctx->d_aps,
-                       ctx->ap_cap, &ctx->d_st->cand_count[r]);
-  }
-  const unsigned long long nchunks =
-      tiles ? (tiles + ctx->opts.chunk_tiles - 1) / ctx->opts.chunk_tiles : 0;
-  // Overlapped form: the chain walk of chunk c runs on a second stream while
-  // the sieve of chunk c+1 fills the other ring.
-  const bool two_streams = overlap && !count_only && nchunks > 1;
-  const bool use_graph = ctx->opts.use_graphs != 0 && !two_streams;
-  const long long key = ((long long)ctx->variant << 40) | ((long long)(count_only ? 1 : 0) << 32) |
-                        (long long)njobs;
-  if (use_graph && (ctx->chunk_graph == nullptr || ctx->graph_key != key)) {
-    if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
-    cudaStream_t cs;
-    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    chunk_begin_kernel<<<1, 1, 0, cs>>>(ctx->d_st, 0);
-    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), cs>>>(sa[0]);
-    if (!count_only) chain_kernel<<<ctx->chain_blocks, kChainThreads, 0, cs>>>(ca[0]);
-    chunk_end_kernel<<<1, 1, 0, cs>>>(ctx->d_st, ctx->cand_cap, 0);
-    cudaError_t ce = cudaStreamEndCapture(cs, &g);
-    cudaStreamDestroy(cs);
-    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
-    ce = cudaGraphInstantiate(&ctx->chunk_graph, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaGraphInstantiate");
-    ctx->graph_key = key;
-  }
-  const bool prof = ctx->opts.profile != 0;
+  memset(S.h_st, 0, sizeof(DevState));
+  S.h_st->chunk_size = (unsigned long long)ctx->opts.chunk_tiles;
+  S.h_st->total_tiles = tiles;
+  S.njobs = njobs;
+  S.count_only = count_only;
+  S.nchunks = tiles ? (tiles + ctx->opts.chunk_tiles - 1) / ctx->opts.chunk_tiles : 0;
+  const bool two_streams = overlap && !count_only && S.nchunks > 1;
   // sieve launches timed with events: the first kProfChunks chunks at most
   constexpr unsigned long long kProfChunks = 4096;
-  const unsigned long long nprof = prof ? std::min(nchunks, kProfChunks) : 0;
-  if ((unsigned long long)ctx->prof_events.size() < 2 * nprof) {
-    for (size_t i = ctx->prof_events.size(); i < 2 * nprof; i++) {
-      cudaEvent_t e;
-      CK(cudaEventCreate(&e));
-      ctx->prof_events.push_back(e);
-    }
-  }
-  for (unsigned long long c = 0; c < nchunks; c++) {
-    const int r = two_streams ? (int)(c & 1) : 0;
-    if (use_graph && !prof) {
-      CK(cudaGraphLaunch(ctx->chunk_graph, s));
-    } else {
-      // ring r is free once the chain walk of chunk c-2 has read it
-      if (two_streams && c >= 2) CK(cudaStreamWaitEvent(s, ctx->chain_done[r], 0));
-      chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st, r);
-      if (c < nprof) CK(cudaEventRecord(ctx->prof_events[2 * c], s));
-      V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa[r]);
-      if (c < nprof) CK(cudaEventRecord(ctx->prof_events[2 * c + 1], s));
-      if (two_streams) {
-        chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap, r);
-        CK(cudaEventRecord(ctx->sieve_done[r], s));
-        CK(cudaStreamWaitEvent(ctx->stream2, ctx->sieve_done[r], 0));
-        chain_kernel<<<ctx->chain_blocks, kChainThreads, 0, ctx->stream2>>>(ca[r]);
-        CK(cudaEventRecord(ctx->chain_done[r], ctx->stream2));
-      } else {
-        if (!count_only) chain_kernel<<<ctx->chain_blocks, kChainThreads, 0, s>>>(ca[r]);
-        chunk_end_kernel<<<1, 1, 0, s>>>(ctx->d_st, ctx->cand_cap, r);
+  S.nprof = (ctx->opts.profile && &S == &ctx->main) ? std::min(S.nchunks, kProfChunks) : 0;
+  if ((rc = ensure_prof_events(ctx, S.nprof)) != AP26_OK) return rc;
+  S.launches = 1 + (int)S.nchunks * (count_only ? 3 : 4) + (count_only ? 0 : 1);
+  CK(cudaEventRecord(S.t0, ctx->stream));
+  bool launched = false;
+  if (ctx->opts.use_graphs > 0) {
+    const long long key[7] = {(long long)(uintptr_t)&S, ctx->variant, njobs,
+                              (long long)S.nchunks, ctx->opts.chunk_tiles,
+                              (count_only ? 1 : 0) | (two_streams ? 2 : 0) | (build_tables ? 4 : 0) |
+                                  ((long long)S.nprof << 3),
+                              (long long)(uintptr_t)tables};
+    GraphEntry *hit = nullptr;
+    for (auto &g : ctx->graphs)
+      if (!memcmp(g.key, key, sizeof(key))) hit = &g;
+    if (!hit) {
+      cudaGraphExec_t exec = nullptr;
+      if (capture_run(ctx, S, tables, build_tables, two_streams, &exec) == cudaSuccess) {
+        if (ctx->graphs.size() >= kMaxGraphs) {   // evict the least recently used
+          auto lru = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                      [](const GraphEntry &a, const GraphEntry &b) {
+                                        return a.used < b.used;
+                                      });
+          cudaGraphExecDestroy(lru->exec);
+          ctx->graphs.erase(lru);
+        }
+        GraphEntry g;
+        memcpy(g.key, key, sizeof(key));
+        g.exec = exec;
+        g.used = 0;
+        ctx->graphs.push_back(g);
+        hit = &ctx->graphs.back();
       }
-      CK(cudaGetLastError());
     }
-    launches += count_only ? 3 : 4;
+    if (hit) {
+      hit->used = ++ctx->graph_clock;
+      CK(cudaGraphLaunch(hit->exec, ctx->stream));
+      launched = true;
+    }
   }
-  if (two_streams) {   // the last chain walks must finish before the read-back
-    CK(cudaStreamWaitEvent(s, ctx->chain_done[0], 0));
-    CK(cudaStreamWaitEvent(s, ctx->chain_done[1], 0));
-  }
-  if (!count_only) {
-    // ReportSolution of every report on the device (AP26.cpp:549-602)
-    ReportArgs ra;
-    ra.aps = ctx->d_aps;
-    ra.count = &ctx->d_st->ap_count;
-    ra.n = ctx->ap_cap;
-    ra.jobs = ctx->d_jobs;
-    ra.fin = ctx->d_fin;
-    ra.job_hash = ctx->d_job_hash;
-    report_kernel<<<ctx->num_sms * 2, REPORT_WARPS * 32, 0, s>>>(ra);
-    CK(cudaGetLastError());
-    launches++;
-  }
-  CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(ctx->h_job_counts, ctx->d_job_counts, sizeof(unsigned long long) * njobs,
-                     cudaMemcpyDeviceToHost, s));
-  if (!count_only)
-    CK(cudaMemcpyAsync(ctx->h_job_hash, ctx->d_job_hash, sizeof(unsigned long long) * njobs,
-                       cudaMemcpyDeviceToHost, s));
-  CK(cudaEventRecord(ctx->ev1, s));
-  if ((rc = wait_stream(ctx, ctx->opts.wait_timeout_s)) != AP26_OK) return rc;
-  long long n_aps = (long long)std::min<unsigned long long>(ctx->h_st->ap_count, ctx->ap_cap);
+  if (!launched) CK(emit_run(ctx, S, tables, build_tables, two_streams, false));
+  if (record_done) CK(cudaEventRecord(S.done, ctx->stream));
+  return AP26_OK;
+}
+
+// Reads back the reports of a finished run (S.done has fired) with one copy
+// on `cs`, and fills stats.
+static int collect_run(ap26_ctx *ctx, JobSet &S, cudaStream_t cs, ap26_stats *stats,
+                       long long *n_aps_out) {
+  long long n_aps = (long long)std::min<unsigned long long>(S.h_st->ap_count, S.ap_cap);
   if (n_aps > 0) {
-    CK(cudaMemcpyAsync(ctx->h_aps, ctx->d_aps, sizeof(APRec) * n_aps, cudaMemcpyDeviceToHost, s));
-    if (!count_only)
-      CK(cudaMemcpyAsync(ctx->h_fin, ctx->d_fin, sizeof(FinRec) * n_aps, cudaMemcpyDeviceToHost,
-                         s));
-    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyAsync(S.h_aps, S.d_aps, sizeof(APRec) * n_aps, cudaMemcpyDeviceToHost, cs));
+    if (!S.count_only)
+      CK(cudaMemcpyAsync(S.h_fin, S.d_fin, sizeof(FinRec) * n_aps, cudaMemcpyDeviceToHost, cs));
+    CK(cudaStreamSynchronize(cs));
   }
-  float ms = 0;
-  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   if (stats) {
     memset(stats, 0, sizeof(*stats));
-    stats->candidates = (int64_t)ctx->h_st->cand_total;
-    stats->late_items = (int64_t)ctx->h_st->late_items;
-    stats->prp_tests = (int64_t)ctx->h_st->prp_tests;
-    stats->aps = (int64_t)ctx->h_st->ap_count;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, S.t0, S.done);
+    stats->candidates = (int64_t)S.h_st->cand_total;
+    stats->late_items = (int64_t)S.h_st->late_items;
+    stats->prp_tests = (int64_t)S.h_st->prp_tests;
+    stats->aps = (int64_t)S.h_st->ap_count;
     stats->device_ms = ms;
-    stats->error_flags = (int32_t)ctx->h_st->err_flags;
-    stats->launches = launches;
+    stats->error_flags = (int32_t)S.h_st->err_flags;
+    stats->launches = S.launches;
     int64_t n53 = 0;
-    for (int j = 0; j < njobs; j++) n53 += ctx->h_jobs[j].q_end - ctx->h_jobs[j].q_begin;
+    for (int j = 0; j < S.njobs; j++) n53 += S.h_jobs[j].q_end - S.h_jobs[j].q_begin;
     stats->sieve_cells = n53 * J59 * WORDS;
-    stats->sieve_launches = (int32_t)nchunks;
-    if (prof) {
-      if (nprof < nchunks) {
+    stats->sieve_launches = (int32_t)S.nchunks;
+    if (S.nprof) {
+      if (S.nprof < S.nchunks) {
         // only the first nprof chunks were timed; all of them are full
-        stats->sieve_cells = (int64_t)(nprof * (unsigned long long)ctx->opts.chunk_tiles) *
+        const int64_t tile_n53 = (int64_t)kVariants[ctx->variant].WARPS * 32;
+        stats->sieve_cells = (int64_t)(S.nprof * (unsigned long long)ctx->opts.chunk_tiles) *
                              tile_n53 * J59 * WORDS;
-        stats->sieve_launches = (int32_t)nprof;
+        stats->sieve_launches = (int32_t)S.nprof;
       }
       double sm = 0;
-      for (unsigned long long c = 0; c < nprof; c++) {
+      for (unsigned long long c = 0; c < S.nprof; c++) {
         float t = 0;
         cudaEventElapsedTime(&t, ctx->prof_events[2 * c], ctx->prof_events[2 * c + 1]);
         sm += t;
       }
       stats->sieve_ms = sm;
     }
-  }
-  if (count_only) {
-    // count-only runs have no candidate buffer use: totals come from job counts
-    unsigned long long tot = 0;
-    for (int j = 0; j < njobs; j++) tot += ctx->h_job_counts[j];
-    if (stats) stats->candidates = (int64_t)tot;
+    if (S.count_only) {
+      // count-only runs have no candidate buffer use: totals come from job counts
+      unsigned long long tot = 0;
+      for (int j = 0; j < S.njobs; j++) tot += S.h_job_counts[j];
+      stats->candidates = (int64_t)tot;
+    }
   }
   if (n_aps_out) *n_aps_out = n_aps;
-  const unsigned err = ctx->h_st->err_flags;
+  const unsigned err = S.h_st->err_flags;
   if (err & ERR_DOMAIN) {
     ctx->last_error = "chain term reached 2^62";
     return AP26_E_DOMAIN;
@@ -795,6 +985,16 @@ static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats
     return AP26_E_OVERFLOW;
   }
   return AP26_OK;
+}
+
+// Synchronous run on the main job set.
+static int run_jobs(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
+                    long long *n_aps_out, bool overlap = false) {
+  int rc;
+  drain(ctx);
+  if ((rc = enqueue_jobs(ctx, ctx->main, njobs, count_only, overlap)) != AP26_OK) return rc;
+  if ((rc = wait_event(ctx, ctx->main.done, ctx->opts.wait_timeout_s)) != AP26_OK) return rc;
+  return collect_run(ctx, ctx->main, ctx->stream, stats, n_aps_out);
 }
 
 static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1,
@@ -812,28 +1012,24 @@ static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1
 static int run_jobs_retry(ap26_ctx *ctx, int njobs, bool count_only, ap26_stats *stats,
                           long long *n_aps, bool overlap = false) {
   const int saved = ctx->opts.chunk_tiles;
-  std::vector<KJob> keep(ctx->h_jobs, ctx->h_jobs + njobs);
+  std::vector<KJob> keep(ctx->main.h_jobs, ctx->main.h_jobs + njobs);
   int rc = run_jobs(ctx, njobs, count_only, stats, n_aps, overlap);
   int tries = 0;
-  while (rc == AP26_E_OVERFLOW && (ctx->h_st->err_flags & ERR_CAND_OVERFLOW) &&
+  while (rc == AP26_E_OVERFLOW && (ctx->main.h_st->err_flags & ERR_CAND_OVERFLOW) &&
          ctx->opts.chunk_tiles > 64 && tries < 6) {
     ctx->opts.chunk_tiles /= 4;
-    if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
-    memcpy(ctx->h_jobs, keep.data(), sizeof(KJob) * njobs);
+    memcpy(ctx->main.h_jobs, keep.data(), sizeof(KJob) * njobs);
     rc = run_jobs(ctx, njobs, count_only, stats, n_aps, overlap);
     if (stats) stats->error_flags |= 1;
     tries++;
   }
-  if (ctx->opts.chunk_tiles != saved) {
-    ctx->opts.chunk_tiles = saved;
-    if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
-  }
+  ctx->opts.chunk_tiles = saved;
   return rc;
 }
 
-static void aprec_to_ap(const ap26_ctx *ctx, const APRec &r, ap26_ap &a) {
+static void aprec_to_ap(const JobSet &S, const APRec &r, ap26_ap &a) {
   a.k = r.k;
-  a.K = ctx->h_jobs[r.job].K;
+  a.K = S.h_jobs[r.job].K;
   a.first = r.first;
   a.n = r.n;
 }
@@ -847,34 +1043,26 @@ static_assert(REP_INVALID == AP26_E_INVALID && REP_DOMAIN == AP26_E_DOMAIN &&
                   REP_ARG == AP26_E_ARG && REP_OVERFLOW == AP26_E_OVERFLOW,
               "report status codes are the public ones");
 
-constexpr long long kMaxIntV = 2000000000;   // MAXINTV, AP26.cpp:88
-
-// result_hash after adding `add` through ReportSolution calls, each of which
-// adds first%1000 + len and subtracts MAXINTV when above it (AP26.cpp:556-560):
-// for a start in [0, MAXINTV] the value stays in [0, MAXINTV], is congruent
-// to the total and is 0 only for a zero total.
-static int32_t hash_fold(int32_t h0, unsigned long long add) {
-  const unsigned long long total = (unsigned long long)h0 + add;
-  if (total == 0) return 0;
-  return (int32_t)((total - 1) % (unsigned long long)kMaxIntV + 1);
-}
-
 // A report with its ReportSolution result and AVX2 order key.
 struct RepOut {
   ap26_ap ap;
   FinRec fin;
   uint64_t key;
+  int word;
 };
 
-// Reports of run_jobs' last call, job index alongside.
-static std::vector<std::pair<int, RepOut>> collect_reports(const ap26_ctx *ctx, long long n) {
+// Reports of a finished run, job index alongside.
+static std::vector<std::pair<int, RepOut>> collect_reports(const JobSet &S, long long n) {
   std::vector<std::pair<int, RepOut>> v((size_t)n);
   for (long long i = 0; i < n; i++) {
-    const APRec &r = ctx->h_aps[i];
+    const APRec &r = S.h_aps[i];
     v[i].first = r.job;
-    aprec_to_ap(ctx, r, v[i].second.ap);
-    v[i].second.fin = ctx->h_fin[i];
-    v[i].second.key = ap26h_order_key(v[i].second.ap.K, ctx->h_jobs[r.job].shift, r.n);
+    aprec_to_ap(S, r, v[i].second.ap);
+    v[i].second.fin = S.h_fin[i];
+    const int shift = S.h_jobs[r.job].shift;
+    v[i].second.key = ap26h_order_key(v[i].second.ap.K, shift, r.n);
+    const int t = (int)((uint64_t)r.n / (uint64_t)MOD) - shift;
+    v[i].second.word = std::min(std::max(t >> 6, 0), WORDS - 1);
   }
   return v;
 }
@@ -894,20 +1082,23 @@ extern "C" int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int 
   if (!ap26_will_search(K)) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
-  fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K);
+  int rc;
+  if ((rc = jobset_ensure(ctx, ctx->main, 1)) != AP26_OK) return rc;
+  fill_job(ctx->main.h_jobs[0], K, shift, 0, 0, N53_PER_K);
   long long n = 0;
-  int rc = run_jobs_retry(ctx, 1, false, stats, &n);
+  rc = run_jobs_retry(ctx, 1, false, stats, &n);
   if (rc != AP26_OK) return rc;
   *n_out = (int)n;
   if (n > cap) return AP26_E_CAPACITY;
-  for (long long i = 0; i < n; i++) aprec_to_ap(ctx, ctx->h_aps[i], out[i]);
+  for (long long i = 0; i < n; i++) aprec_to_ap(ctx->main, ctx->main.h_aps[i], out[i]);
   ap26_sort_aps(out, (int)n, shift);
   return AP26_OK;
 }
 
-extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
-                                 int32_t *result_hash, ap26_sol *sol, int cap, int *n_sol,
-                                 ap26_stats *stats) {
+extern "C" int ap26_search_k_sol_words(ap26_ctx *ctx, int K, int shift, int iter,
+                                       int32_t *result_hash, int32_t *hash_at_word,
+                                       ap26_sol *sol, int32_t *sol_word, int cap, int *n_sol,
+                                       ap26_stats *stats) {
   if (!ctx || !result_hash || !n_sol || cap < 0 || (cap > 0 && !sol)) return AP26_E_ARG;
   if (iter < 0 || iter >= WORDS) return AP26_E_ARG;
   if (*result_hash < 0 || *result_hash > kMaxIntV) return AP26_E_ARG;
@@ -915,11 +1106,13 @@ extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
   if (!ap26_will_search(K)) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
-  fill_job(ctx->h_jobs[0], K, shift, 0, 0, N53_PER_K, iter);
+  int rc;
+  if ((rc = jobset_ensure(ctx, ctx->main, 1)) != AP26_OK) return rc;
+  fill_job(ctx->main.h_jobs[0], K, shift, 0, 0, N53_PER_K, iter);
   long long n = 0;
-  int rc = run_jobs_retry(ctx, 1, false, stats, &n);
+  rc = run_jobs_retry(ctx, 1, false, stats, &n);
   if (rc != AP26_OK) return rc;
-  auto v = collect_reports(ctx, n);
+  auto v = collect_reports(ctx->main, n);
   std::sort(v.begin(), v.end(),
             [](const std::pair<int, RepOut> &x, const std::pair<int, RepOut> &y) {
               return rep_less(x.second, y.second);
@@ -940,10 +1133,24 @@ extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
       sol[o].len = r.second.fin.sol_len[i];
       sol[o].K = K;
       sol[o].first = r.second.fin.sol_first[i];
+      if (sol_word) sol_word[o] = r.second.word;
       o++;
     }
-  *result_hash = hash_fold(*result_hash, ctx->h_job_hash[0]);
+  // per-word progress: the hash after the reports of words iter..w
+  unsigned long long acc = 0;
+  for (int w = 0; w < WORDS; w++) {
+    acc += ctx->main.h_job_hash[w];
+    if (hash_at_word) hash_at_word[w] = w < iter ? *result_hash : hash_fold(*result_hash, acc);
+  }
+  *result_hash = hash_fold(*result_hash, job_hash_total(ctx->main, 0));
   return AP26_OK;
+}
+
+extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
+                                 int32_t *result_hash, ap26_sol *sol, int cap, int *n_sol,
+                                 ap26_stats *stats) {
+  return ap26_search_k_sol_words(ctx, K, shift, iter, result_hash, nullptr, sol, nullptr, cap,
+                                 n_sol, stats);
 }
 
 // ---- batched persistent form ------------------------------------------------------
@@ -962,9 +1169,9 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
       if (ap26_will_search(K)) jobs.push_back({i, K});
   }
   int rc;
-  if ((rc = ensure_jobs(ctx, (int)jobs.size())) != AP26_OK) return rc;
+  if ((rc = jobset_ensure(ctx, ctx->main, (int)jobs.size())) != AP26_OK) return rc;
   for (size_t j = 0; j < jobs.size(); j++)
-    fill_job(ctx->h_jobs[j], jobs[j].second, items[jobs[j].first].shift, jobs[j].first, 0,
+    fill_job(ctx->main.h_jobs[j], jobs[j].second, items[jobs[j].first].shift, jobs[j].first, 0,
              N53_PER_K);
   long long n = 0;
   if (!jobs.empty()) {
@@ -973,12 +1180,13 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
   } else if (stats) {
     memset(stats, 0, sizeof(*stats));
   }
+  const JobSet &S = ctx->main;
   // group reports: item, K ascending, AVX2 order inside K
   std::vector<std::vector<RepOut>> per_item(n_items);
-  for (auto &r : collect_reports(ctx, n)) per_item[ctx->h_jobs[r.first].item].push_back(r.second);
+  for (auto &r : collect_reports(S, n)) per_item[S.h_jobs[r.first].item].push_back(r.second);
   int64_t total = 0;
   std::vector<unsigned long long> hash_add(n_items, 0);
-  for (size_t j = 0; j < jobs.size(); j++) hash_add[jobs[j].first] += ctx->h_job_hash[j];
+  for (size_t j = 0; j < jobs.size(); j++) hash_add[jobs[j].first] += job_hash_total(S, (int)j);
   for (int i = 0; i < n_items; i++) {
     auto &v = per_item[i];
     std::sort(v.begin(), v.end(), rep_less);
@@ -995,7 +1203,7 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
     total += (int64_t)v.size();
   }
   for (size_t j = 0; j < jobs.size(); j++) {
-    res[jobs[j].first].candidates += (int64_t)ctx->h_job_counts[j];
+    res[jobs[j].first].candidates += (int64_t)S.h_job_counts[j];
     res[jobs[j].first].ks_searched++;
   }
   *n_aps = total;
@@ -1006,94 +1214,277 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
 }
 
 // ---- serving: continuous batching ----------------------------------------------------
-// A unit costs its K-job tables and descriptors while admitted.
-static int64_t unit_bytes(size_t nk) { return (int64_t)nk * (TABLE_WORDS * 4 + sizeof(KJob) + 8); }
+// Device memory a serving context holds.  Fixed: the two slices' job sets
+// (descriptors, counters, hash sums, 2^16 reports each) and the unit slots;
+// the candidate rings are the context's own and shared with every other
+// form.  Per admitted unit: one table (the sieve bitstrings of one K) per
+// searchable K still to search.  The pool of tables is allocated at the first
+// admission, sized from opts.mem_budget (default: half of the device memory
+// free at that moment, at most 8 GiB), so a unit is admitted only while its
+// tables fit in memory the device really had.
+constexpr int kSliceJobs = 4;          // K-jobs per serving slice
+constexpr int64_t kTableBytes = (int64_t)TABLE_WORDS * 4;
 
-extern "C" int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item) {
+static int64_t slice_set_bytes() {
+  const int64_t jobs = 64;   // jobset_ensure's minimum capacity
+  return jobs * ((int64_t)sizeof(KJob) + 8 + 8 * WORDS) + (int64_t)sizeof(DevState) +
+         (1ll << 16) * (int64_t)(sizeof(APRec) + sizeof(FinRec));
+}
+
+static int serve_pool_init(ap26_ctx *ctx) {
+  if (ctx->d_pool) return AP26_OK;
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  int64_t budget = ctx->opts.mem_budget;
+  if (budget <= 0) budget = std::min<int64_t>((int64_t)(free_b / 2), (int64_t)8 << 30);
+  budget = std::min<int64_t>(budget, (int64_t)free_b);
+  const int64_t fixed = 2 * slice_set_bytes() + (int64_t)sizeof(UnitState) * kUnitSlots;
+  const int64_t n = (budget - fixed) / kTableBytes;
+  if (n < 1) {
+    ctx->last_error = "serving memory budget below its fixed buffers";
+    return AP26_E_NOMEM;
+  }
+  CK(cudaMalloc(&ctx->d_pool, (size_t)n * kTableBytes));
+  ctx->pool_tables = (int)std::min<int64_t>(n, INT32_MAX);
+  ctx->serve_budget = fixed + n * kTableBytes;
+  ctx->bytes_in_use = fixed;
+  ctx->free_tables.clear();
+  for (int i = ctx->pool_tables - 1; i >= 0; i--) ctx->free_tables.push_back(i);
+  for (int i = 0; i < 2; i++) {
+    int rc = jobset_ensure(ctx, ctx->slices[i].set, kSliceJobs);
+    if (rc != AP26_OK) return rc;
+    CK(cudaMalloc(&ctx->slices[i].d_snap, sizeof(UnitState) * kSliceJobs));
+    CK(cudaMallocHost(&ctx->slices[i].h_snap, sizeof(UnitState) * kSliceJobs));
+  }
+  return AP26_OK;
+}
+
+static int serve_admit(ap26_ctx *ctx, const ap26_item *item, int K_start, int iter,
+                       int32_t h0) {
   if (!ctx || !item || item->kmax < item->kmin) return AP26_E_ARG;
   if (!k_in_domain(item->kmin, item->shift) || !k_in_domain(item->kmax, item->shift))
     return AP26_E_DOMAIN;
+  if (iter < 0 || iter >= WORDS || h0 < 0 || h0 > kMaxIntV) return AP26_E_ARG;
+  if (K_start < item->kmin || K_start > item->kmax + 1) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = serve_pool_init(ctx)) != AP26_OK) return rc;
   ServeUnit u;
   u.item = *item;
-  for (int K = item->kmin; K <= item->kmax; K++)
+  for (int K = K_start; K <= item->kmax; K++)
     if (ap26_will_search(K)) u.ks.push_back(K);
-  const int64_t need = unit_bytes(u.ks.size());
-  if (ctx->bytes_in_use + need > ctx->opts.mem_budget || ctx->free_slots.empty())
+  u.iter0 = (!u.ks.empty() && u.ks[0] == K_start) ? iter : 0;
+  u.bytes = (int64_t)u.ks.size() * kTableBytes;
+  if (ctx->free_slots.empty() || u.ks.size() > ctx->free_tables.size()) {
+    ctx->last_error = "serving memory budget exceeded";
     return AP26_E_NOMEM;
-  CK(cudaSetDevice(ctx->device));
+  }
+  for (size_t i = 0; i < u.ks.size(); i++) {
+    u.tables.push_back(ctx->free_tables.back());
+    ctx->free_tables.pop_back();
+  }
   u.slot = ctx->free_slots.back();
-  CK(cudaMemsetAsync(ctx->d_units + u.slot, 0, sizeof(UnitState), ctx->stream));
   ctx->free_slots.pop_back();
-  ctx->bytes_in_use += need;
+  ctx->bytes_in_use += u.bytes;
+  // the unit's checkpoint and tables go to the device now, on the pipeline
+  // stream, ahead of every slice that can use them
+  UnitState &us = u.snap;
+  memset(&us, 0, sizeof(us));
+  us.K_next = K_start;
+  us.iter = u.iter0;
+  us.result_hash = h0;
+  us.h0 = h0;
+  us.kmin = item->kmin;
+  us.kmax = item->kmax;
+  us.shift = item->shift;
+  size_t i = 0;
+  do {
+    AdmitArgs a;
+    memset(&a, 0, sizeof(a));
+    a.init = us;
+    a.slot = u.slot;
+    a.write_init = i == 0;
+    a.shift = item->shift;
+    a.n = (int)std::min<size_t>(kAdmitMax, u.ks.size() - i);
+    for (int b = 0; b < a.n; b++) {
+      a.K[b] = u.ks[i + b];
+      a.table[b] = u.tables[i + b];
+    }
+    admit_unit_kernel<<<std::max(1, a.n), 256, 0, ctx->stream>>>(a, ctx->d_units, ctx->d_pool);
+    CK(cudaGetLastError());
+    i += (size_t)a.n;
+  } while (i < u.ks.size());
   u.t_submit = std::chrono::steady_clock::now();
   ctx->units.push_back(std::move(u));
   return AP26_OK;
 }
 
-// One slice: up to `slice_k` K-jobs drawn round-robin from the admitted units
-// run as one batched launch chain; finished units move to the poll queue.
-extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
-  if (!ctx) return AP26_E_ARG;
-  CK(cudaSetDevice(ctx->device));
-  drain(ctx);
-  // One K-job per admitted unit per slice (round-robin), at most 8: a slice
-  // then lasts about one K of device time however many units are waiting,
-  // and a unit that arrives during a slice starts with the next one.
-  const int slice_k = std::max(1, std::min<int>(8, (int)ctx->units.size()));
-  std::vector<std::pair<ServeUnit *, int>> picked;
+extern "C" int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item) {
+  if (!item) return AP26_E_ARG;
+  return serve_admit(ctx, item, item->kmin, 0, 0);
+}
+
+extern "C" int ap26_serve_submit_from(ap26_ctx *ctx, const ap26_item *item, int K, int ITER,
+                                      int32_t result_hash) {
+  return serve_admit(ctx, item, K, ITER, result_hash);
+}
+
+static ServeUnit *find_unit(ap26_ctx *ctx, int64_t id) {
+  for (auto &u : ctx->units)
+    if (u.item.id == id) return &u;
+  return nullptr;
+}
+
+// Folds a finished slice into its units: reports (host), progress.
+static int harvest_slice(ap26_ctx *ctx, Slice &sl) {
+  JobSet &S = sl.set;
+  long long n = 0;
+  int rc = sl.rc;
+  if (rc == AP26_OK) rc = collect_run(ctx, S, ctx->copy_stream, nullptr, &n);
+  std::vector<std::vector<RepOut>> per_job(S.njobs);
+  if (rc == AP26_OK)
+    for (auto &r : collect_reports(S, n)) per_job[r.first].push_back(r.second);
+  for (int j = 0; j < S.njobs; j++) {
+    ServeUnit *u = find_unit(ctx, sl.unit_ids[j]);
+    if (!u) continue;
+    if (rc != AP26_OK) {
+      if (u->status == AP26_OK) u->status = rc;
+      continue;
+    }
+    std::sort(per_job[j].begin(), per_job[j].end(), rep_less);
+    for (const auto &r : per_job[j]) {
+      u->aps.push_back(r.ap);
+      if (r.fin.status != AP26_OK && u->status == AP26_OK) u->status = r.fin.status;
+    }
+    u->done_k++;
+    // slices finish in order and this one holds the unit's latest state
+    u->snap = sl.h_snap[j];
+  }
+  sl.busy = false;
+  return rc;
+}
+
+// Builds and enqueues one slice: up to kSliceJobs K-jobs, one per admitted
+// unit per round (round-robin), each unit's K in ascending order.
+static int launch_slice(ap26_ctx *ctx, Slice &sl) {
+  std::vector<std::pair<ServeUnit *, size_t>> picked;
   bool progress = true;
-  while ((int)picked.size() < slice_k && progress) {
+  while ((int)picked.size() < kSliceJobs && progress) {
     progress = false;
     for (auto &u : ctx->units) {
-      if ((int)picked.size() >= slice_k) break;
-      if (u.next_k < u.ks.size()) {
-        picked.push_back({&u, u.ks[u.next_k++]});
+      if ((int)picked.size() >= kSliceJobs) break;
+      if (u.status == AP26_OK && u.next_k < u.ks.size()) {
+        picked.push_back({&u, u.next_k++});
         progress = true;
       }
     }
   }
-  if (!picked.empty()) {
-    int rc;
-    if ((rc = ensure_jobs(ctx, (int)picked.size())) != AP26_OK) return rc;
-    for (size_t j = 0; j < picked.size(); j++)
-      fill_job(ctx->h_jobs[j], picked[j].second, picked[j].first->item.shift,
-               picked[j].first->slot, 0, N53_PER_K);
-    long long n = 0;
-    ap26_stats st;
-    rc = run_jobs_retry(ctx, (int)picked.size(), false, &st, &n, true);
-    if (rc != AP26_OK) {
-      for (auto &pk : picked) pk.first->status = rc;
-    } else {
-      // the units' running sums stay on the device
-      unit_accumulate_kernel<<<1, 256, 0, ctx->stream>>>(ctx->d_jobs, (int)picked.size(),
-                                                         ctx->d_job_counts, ctx->d_job_hash,
-                                                         ctx->d_units);
-      CK(cudaGetLastError());
-      std::vector<std::vector<RepOut>> per_job(picked.size());
-      for (auto &r : collect_reports(ctx, n)) per_job[r.first].push_back(r.second);
-      for (size_t j = 0; j < picked.size(); j++) {
-        ServeUnit *u = picked[j].first;
-        std::sort(per_job[j].begin(), per_job[j].end(), rep_less);
-        for (const auto &r : per_job[j]) {
-          u->aps.push_back(r.ap);
-          if (r.fin.status != AP26_OK && u->status == AP26_OK) u->status = r.fin.status;
-        }
-        u->done_k++;
-      }
-    }
+  if (picked.empty()) return AP26_OK;
+  JobSet &S = sl.set;
+  int rc;
+  if ((rc = jobset_ensure(ctx, S, (int)picked.size())) != AP26_OK) return rc;
+  sl.unit_ids.clear();
+  for (size_t j = 0; j < picked.size(); j++) {
+    ServeUnit *u = picked[j].first;
+    const size_t i = picked[j].second;
+    fill_job(S.h_jobs[j], u->ks[i], u->item.shift, u->slot, 0, N53_PER_K, i == 0 ? u->iter0 : 0);
+    S.h_jobs[j].table = u->tables[i];
+    sl.unit_ids.push_back(u->item.id);
   }
+  sl.busy = true;
+  sl.rc = enqueue_jobs(ctx, S, (int)picked.size(), false, true, ctx->d_pool, 0, false);
+  if (sl.rc == AP26_OK) {
+    // the units' running sums and checkpoints stay on the device; the slice
+    // reads back its units' states in stream order, then S.done fires
+    unit_accumulate_kernel<<<1, 256, 0, ctx->stream>>>(S.d_jobs, S.njobs, S.d_job_counts,
+                                                       S.d_job_hash, ctx->d_units, sl.d_snap);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sl.h_snap, sl.d_snap, sizeof(UnitState) * S.njobs,
+                          cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(S.done, ctx->stream);
+    if (e != cudaSuccess) sl.rc = cuda_fail(ctx, e, "serving slice");
+  }
+  return sl.rc;
+}
+
+static void retire_units(ap26_ctx *ctx) {
   for (auto it = ctx->units.begin(); it != ctx->units.end();) {
-    if (it->done_k == (int)it->ks.size() || it->status != AP26_OK) {
+    bool in_flight = false;
+    for (int i : ctx->inflight)
+      for (int64_t id : ctx->slices[i].unit_ids)
+        if (id == it->item.id) in_flight = true;
+    const bool done = it->done_k == (int)it->ks.size();
+    if ((done || it->status != AP26_OK) && !in_flight) {
       it->latency_ms = std::chrono::duration<double, std::milli>(
                            std::chrono::steady_clock::now() - it->t_submit).count();
-      ctx->bytes_in_use -= unit_bytes(it->ks.size());
+      for (int t : it->tables) ctx->free_tables.push_back(t);
+      it->tables.clear();
+      ctx->bytes_in_use -= it->bytes;
       ctx->finished.push_back(std::move(*it));
       it = ctx->units.erase(it);
     } else {
       ++it;
     }
   }
+}
+
+// Non-blocking: harvests every finished slice, then keeps two slices in
+// flight while admitted units have K left.  Units submitted while slices run
+// join the next slice that is built.
+extern "C" int ap26_serve_step(ap26_ctx *ctx, int *active_units) {
+  if (!ctx) return AP26_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int rc = AP26_OK;
+  while (!ctx->inflight.empty()) {
+    Slice &sl = ctx->slices[ctx->inflight.front()];
+    cudaError_t q = cudaEventQuery(sl.set.done);
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return cuda_fail(ctx, q, "cudaEventQuery");
+    ctx->inflight.pop_front();
+    int r = harvest_slice(ctx, sl);
+    if (r != AP26_OK && rc == AP26_OK) rc = r;
+  }
+  while (ctx->inflight.size() < 2) {
+    int idx = ctx->slices[0].busy ? 1 : 0;
+    if (ctx->slices[idx].busy) break;
+    int r = launch_slice(ctx, ctx->slices[idx]);
+    if (!ctx->slices[idx].busy) break;   // nothing left to schedule
+    ctx->inflight.push_back(idx);
+    if (r != AP26_OK && rc == AP26_OK) rc = r;
+  }
+  retire_units(ctx);
   if (active_units) *active_units = (int)ctx->units.size();
+  return rc;
+}
+
+// Blocks until the oldest slice in flight has finished (AP26_OK, also when
+// none is in flight) or max_wait_s has passed (AP26_E_TIMEOUT, nothing lost).
+extern "C" int ap26_serve_wait(ap26_ctx *ctx, double max_wait_s) {
+  if (!ctx) return AP26_E_ARG;
+  if (ctx->inflight.empty()) return AP26_OK;
+  CK(cudaSetDevice(ctx->device));
+  int rc = wait_event(ctx, ctx->slices[ctx->inflight.front()].set.done, max_wait_s);
+  if (rc == AP26_E_TIMEOUT) ctx->pending = false;   // the slice is still tracked
+  return rc;
+}
+
+extern "C" int ap26_serve_checkpoint(ap26_ctx *ctx, int64_t id, int *kmin, int *kmax,
+                                     int *shift, int *K, int *ITER, int32_t *result_hash) {
+  if (!ctx || !K || !ITER || !result_hash) return AP26_E_ARG;
+  const ServeUnit *u = find_unit(ctx, id);
+  if (!u)
+    for (const auto &f : ctx->finished)
+      if (f.item.id == id) u = &f;
+  if (!u) return AP26_E_ARG;
+  // the unit's device slot as its last finished slice read it back
+  const UnitState &us = u->snap;
+  if (kmin) *kmin = us.kmin;
+  if (kmax) *kmax = us.kmax;
+  if (shift) *shift = us.shift;
+  *K = us.K_next;
+  *ITER = us.iter;
+  *result_hash = us.result_hash;
   return AP26_OK;
 }
 
@@ -1104,12 +1495,8 @@ extern "C" int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *ap
   ServeUnit &u = ctx->finished.front();
   *n_aps = (int64_t)u.aps.size();
   if ((int64_t)u.aps.size() > ap_cap) return AP26_E_CAPACITY;
-  CK(cudaSetDevice(ctx->device));
-  drain(ctx);
-  UnitState us;
-  CK(cudaMemcpyAsync(&us, ctx->d_units + u.slot, sizeof(us), cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  // its last slice has finished and read its device slot back
+  const UnitState &us = u.snap;
   if (!u.aps.empty()) memcpy(aps, u.aps.data(), sizeof(ap26_ap) * u.aps.size());
   res->id = u.item.id;
   res->status = u.status;
@@ -1121,11 +1508,18 @@ extern "C" int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *ap
   res->first_ap = 0;
   res->candidates = (int64_t)us.candidates;
   res->ks_searched = (int32_t)u.ks.size();
-  res->result_hash = hash_fold(0, us.hash_add);
+  res->result_hash = hash_fold(us.h0, us.hash_add);
   res->latency_ms = u.latency_ms;
   ctx->free_slots.push_back(u.slot);
   ctx->finished.pop_front();
   return 1;
+}
+
+extern "C" int ap26_serve_memory(const ap26_ctx *ctx, int64_t *in_use, int64_t *budget) {
+  if (!ctx) return AP26_E_ARG;
+  if (in_use) *in_use = ctx->bytes_in_use;
+  if (budget) *budget = ctx->serve_budget;
+  return AP26_OK;
 }
 
 // ---- kernel-level entry points ---------------------------------------------------------
@@ -1135,65 +1529,56 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
   if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
-  fill_job(ctx->h_jobs[0], K, shift, 0, q_begin, q_end);
-  // sieve without the chain walk: one chunk covering everything, candidates kept
-  const int saved = ctx->opts.chunk_tiles;
+  JobSet &S = ctx->main;
+  int rc;
+  if ((rc = jobset_ensure(ctx, S, 1)) != AP26_OK) return rc;
+  // set-up and sieve only, in one launch over the whole range, candidates kept
+  fill_job(S.h_jobs[0], K, shift, 0, q_begin, q_end);
   const int64_t tile_n53 = (int64_t)kVariants[ctx->variant].WARPS * 32;
   const int64_t tiles = (q_end - q_begin + tile_n53 - 1) / tile_n53;
-  ctx->opts.chunk_tiles = (int)std::max<int64_t>(1, tiles);
-  if (ctx->chunk_graph) { cudaGraphExecDestroy(ctx->chunk_graph); ctx->chunk_graph = nullptr; }
-  const int saved_graph = ctx->opts.use_graphs;
-  ctx->opts.use_graphs = 0;
-  // run setup + sieve only (no chain) by hand
-  int rc = AP26_OK;
-  {
-    KJob &J = ctx->h_jobs[0];
-    J.ntiles = (int32_t)tiles;
-    J.tile_begin = 0;
-    memset(ctx->h_st, 0, sizeof(DevState));
-    ctx->h_st->chunk_size = (unsigned long long)std::max<int64_t>(1, tiles);
-    ctx->h_st->total_tiles = (unsigned long long)tiles;
-    cudaStream_t s = ctx->stream;
-    const SieveVariant &V = kVariants[ctx->variant];
-    CK(cudaEventRecord(ctx->ev0, s));
-    CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(ctx->d_job_counts, 0, sizeof(unsigned long long), s));
-    setup_jobs_kernel<<<1, 256, 0, s>>>(ctx->d_jobs, 1, ctx->d_tables);
-    chunk_begin_kernel<<<1, 1, 0, s>>>(ctx->d_st, 0);
-    const SieveArgs sa = sieve_args(ctx->d_jobs, 1, ctx->d_tables, ctx->d_st, ctx->d_cand[0],
-                                    ctx->cand_cap, ctx->d_job_counts, 0,
-                                    &ctx->d_st->cand_count[0]);
-    V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-    CK(cudaEventRecord(ctx->ev1, s));
-    rc = wait_stream(ctx, ctx->opts.wait_timeout_s);
-    if (rc == AP26_OK) {
-      const long long nc = (long long)ctx->h_st->cand_count[0];
-      *n_cand = nc;
-      if (nc > ctx->cand_cap) rc = AP26_E_OVERFLOW;
-      else if (nc > cap) rc = AP26_E_CAPACITY;
-      else if (nc > 0) {
-        std::vector<Cand> tmp(nc);
-        CK(cudaMemcpy(tmp.data(), ctx->d_cand[0], sizeof(Cand) * nc, cudaMemcpyDeviceToHost));
-        for (long long i = 0; i < nc; i++) cand[i] = tmp[i].n;
-      }
-      if (stats) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        memset(stats, 0, sizeof(*stats));
-        stats->candidates = nc;
-        stats->late_items = (int64_t)ctx->h_st->late_items;
-        stats->device_ms = ms;
-        stats->error_flags = (int32_t)ctx->h_st->err_flags;
-        stats->launches = 3;
-      }
-    }
+  KJob &J = S.h_jobs[0];
+  J.ntiles = (int32_t)tiles;
+  J.tile_begin = 0;
+  J.table = 0;
+  memset(S.h_st, 0, sizeof(DevState));
+  S.h_st->chunk_size = (unsigned long long)std::max<int64_t>(1, tiles);
+  S.h_st->total_tiles = (unsigned long long)tiles;
+  cudaStream_t s = ctx->stream;
+  const SieveVariant &V = kVariants[ctx->variant];
+  CK(cudaEventRecord(ctx->ev0, s));
+  CK(cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(S.d_st, S.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(S.d_job_counts, 0, sizeof(unsigned long long), s));
+  setup_jobs_kernel<<<1, 256, 0, s>>>(S.d_jobs, 1, S.d_tables, 1);
+  chunk_begin_kernel<<<1, 1, 0, s>>>(S.d_st, 0);
+  const SieveArgs sa = sieve_args(S.d_jobs, 1, S.d_tables, S.d_st, ctx->d_cand[0],
+                                  ctx->cand_cap, S.d_job_counts, 0, &S.d_st->cand_count[0]);
+  V.kernel<<<ctx->sieve_blocks, V.WARPS * 32, V.smem(), s>>>(sa);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(S.h_st, S.d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(ctx->ev1, s));
+  rc = wait_event(ctx, ctx->ev1, ctx->opts.wait_timeout_s);
+  if (rc != AP26_OK) return rc;
+  const long long nc = (long long)S.h_st->cand_count[0];
+  *n_cand = nc;
+  if (nc > ctx->cand_cap) return AP26_E_OVERFLOW;
+  if (nc > cap) return AP26_E_CAPACITY;
+  if (nc > 0) {
+    std::vector<Cand> tmp(nc);
+    CK(cudaMemcpy(tmp.data(), ctx->d_cand[0], sizeof(Cand) * nc, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < nc; i++) cand[i] = tmp[i].n;
   }
-  ctx->opts.chunk_tiles = saved;
-  ctx->opts.use_graphs = saved_graph;
-  return rc;
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    memset(stats, 0, sizeof(*stats));
+    stats->candidates = nc;
+    stats->late_items = (int64_t)S.h_st->late_items;
+    stats->device_ms = ms;
+    stats->error_flags = (int32_t)S.h_st->err_flags;
+    stats->launches = 3;
+  }
+  return AP26_OK;
 }
 
 extern "C" int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int shift,
@@ -1202,14 +1587,14 @@ extern "C" int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int sh
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
   int rc;
-  if ((rc = ensure_jobs(ctx, nK)) != AP26_OK) return rc;
+  if ((rc = jobset_ensure(ctx, ctx->main, nK)) != AP26_OK) return rc;
   for (int i = 0; i < nK; i++) {
     if (!k_in_domain(Ks[i], shift)) return AP26_E_DOMAIN;
-    fill_job(ctx->h_jobs[i], Ks[i], shift, i, 0, N53_PER_K);
+    fill_job(ctx->main.h_jobs[i], Ks[i], shift, i, 0, N53_PER_K);
   }
   rc = run_jobs(ctx, nK, true, stats, nullptr);
   if (rc != AP26_OK) return rc;
-  for (int i = 0; i < nK; i++) counts[i] = (int64_t)ctx->h_job_counts[i];
+  for (int i = 0; i < nK; i++) counts[i] = (int64_t)ctx->main.h_job_counts[i];
   return AP26_OK;
 }
 
@@ -1331,36 +1716,39 @@ extern "C" int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t 
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
   if (count == 0) return AP26_OK;
-  fill_job(ctx->h_jobs[0], K, 0, 0, 0, 0);
+  JobSet &S = ctx->main;
+  int rc;
+  if ((rc = jobset_ensure(ctx, S, 1)) != AP26_OK) return rc;
+  fill_job(S.h_jobs[0], K, 0, 0, 0, 0);
   DevBuf<int64_t> dn, df;
   DevBuf<int32_t> dk;
   CK(dn.alloc(count));
   CK(df.alloc(count));
   CK(dk.alloc(count));
   cudaStream_t s = ctx->stream;
-  memset(ctx->h_st, 0, sizeof(DevState));
-  CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
-  setup_jobs_kernel<<<1, 256, 0, s>>>(ctx->d_jobs, 1, ctx->d_tables);
+  memset(S.h_st, 0, sizeof(DevState));
+  CK(cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(S.d_st, S.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+  setup_jobs_kernel<<<1, 256, 0, s>>>(S.d_jobs, 1, S.d_tables, 0);
   CK(cudaMemcpyAsync(dn.p, n, sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev0, s));
-  chain_explicit_kernel<<<ctx->num_sms * 8, 128, 0, s>>>(ctx->d_jobs, dn.p, count, dk.p, df.p,
-                                                         ctx->d_st);
+  chain_explicit_kernel<<<ctx->num_sms * 8, 128, 0, s>>>(S.d_jobs, dn.p, count, dk.p, df.p,
+                                                         S.d_st);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
   CK(cudaMemcpyAsync(k_out, dk.p, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(first_out, df.p, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(S.h_st, S.d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->device_ms = ms;
-    stats->error_flags = (int32_t)ctx->h_st->err_flags;
+    stats->error_flags = (int32_t)S.h_st->err_flags;
     stats->launches = 2;
   }
-  return (ctx->h_st->err_flags & ERR_DOMAIN) ? AP26_E_DOMAIN : AP26_OK;
+  return (S.h_st->err_flags & ERR_DOMAIN) ? AP26_E_DOMAIN : AP26_OK;
 }
 
 extern "C" int ap26_probe_peaks(ap26_ctx *ctx, double *smem_gbs, double *int_tops) {
@@ -1396,38 +1784,58 @@ extern "C" int ap26_probe_peaks(ap26_ctx *ctx, double *smem_gbs, double *int_top
 }
 
 // ---- autotuner -------------------------------------------------------------------------------
-// Times every compiled sieve variant (and two chunk sizes) on the same slice
-// of K's lattice (count-only, so only the sieve is measured) and keeps the
-// fastest.  The slice is the first 1/64 of the K's starts.
+// Two stages.  (1) Every compiled sieve variant (dense primes, tail group,
+// late stage, queue depth, CTA size) on the same slice of K's lattice, the
+// first 1/64 of its starts, count-only in one launch, so only the sieve is
+// timed.  (2) For the fastest variant, the whole pipeline (sieve, chain walk
+// on the second stream, ReportSolution) over one whole K at each chunk size
+// the candidate rings can hold: a chunk is the unit the chain walk overlaps
+// and each chunk boundary drains the persistent sieve once.
 extern "C" int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen) {
   if (!ctx) return AP26_E_ARG;
-  if (!k_in_domain(K, shift)) return AP26_E_DOMAIN;
+  if (!k_in_domain(K, shift) || !ap26_will_search(K)) return AP26_E_DOMAIN;
+  if (!serving_idle(ctx)) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
+  int rc;
+  if ((rc = jobset_ensure(ctx, ctx->main, 1)) != AP26_OK) return rc;
   const int64_t q1 = N53_PER_K / 64;
+  const int saved_chunk = ctx->opts.chunk_tiles;
+  ctx->opts.chunk_tiles = 1 << 20;   // the slice in one launch
   double best_ms = 1e30;
-  int best_v = ctx->variant, best_chunk = ctx->opts.chunk_tiles;
-  const int chunks[2] = {8192, 32768};
+  int best_v = ctx->variant;
   for (int vi = 0; vi < kNumVariants; vi++) {
-    int rc = set_variant(ctx, vi);
-    if (rc != AP26_OK) return rc;
-    for (int ci = 0; ci < 2; ci++) {
-      ctx->opts.chunk_tiles = chunks[ci];
-      double t = 0;
-      for (int rep = 0; rep < 2; rep++) {
-        fill_job(ctx->h_jobs[0], K, shift, 0, 0, q1);
-        ap26_stats st;
-        rc = run_jobs(ctx, 1, true, &st, nullptr);
-        if (rc != AP26_OK) return rc;
-        if (rep == 1) t = st.device_ms;   // first run warms up
-      }
-      if (t < best_ms) { best_ms = t; best_v = vi; best_chunk = chunks[ci]; }
+    if ((rc = set_variant(ctx, vi)) != AP26_OK) return rc;
+    double t = 0;
+    for (int rep = 0; rep < 2; rep++) {
+      fill_job(ctx->main.h_jobs[0], K, shift, 0, 0, q1);
+      ap26_stats st;
+      rc = run_jobs(ctx, 1, true, &st, nullptr);
+      if (rc != AP26_OK) { ctx->opts.chunk_tiles = saved_chunk; return rc; }
+      if (rep == 1) t = st.device_ms;   // first run warms up
     }
+    if (t < best_ms) { best_ms = t; best_v = vi; }
   }
-  int rc = set_variant(ctx, best_v);
+  if ((rc = set_variant(ctx, best_v)) != AP26_OK) return rc;
+  // chunk sizes whose worst-case survivors (about 115 per tile) fit a ring
+  const int tile_n53 = kVariants[best_v].WARPS * 32;
+  int best_chunk = saved_chunk;
+  best_ms = 1e30;
+  for (int chunk = 32768; chunk <= (1 << 20); chunk *= 2) {
+    if ((long long)chunk * 115 * tile_n53 / 256 > ctx->cand_cap) break;
+    ctx->opts.chunk_tiles = chunk;
+    fill_job(ctx->main.h_jobs[0], K, shift, 0, 0, N53_PER_K);
+    ap26_stats st;
+    long long n = 0;
+    rc = run_jobs(ctx, 1, false, &st, &n, true);
+    if (rc == AP26_E_OVERFLOW) break;
+    if (rc != AP26_OK) { ctx->opts.chunk_tiles = saved_chunk; return rc; }
+    if (st.device_ms < best_ms) { best_ms = st.device_ms; best_chunk = chunk; }
+  }
   ctx->opts.chunk_tiles = best_chunk;
+  drop_graphs(ctx);
   if (chosen) *chosen = ctx->opts;
-  return rc;
+  return AP26_OK;
 }
 
 // ---- allocation-free survivor counts ----------------------------------------------------
@@ -1471,6 +1879,7 @@ __global__ void noalloc_init_kernel(NoallocScratch *s, const int32_t *Ks, int nK
     J.q_begin = 0;
     J.q_end = ok ? N53_PER_K : 0;
     J.ntiles = ok ? (int32_t)ntiles : 0;
+    J.table = j;
     s_tiles[j] = J.ntiles;
     s->counts[j] = 0;
   }
@@ -1564,7 +1973,7 @@ extern "C" int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK,
     do {
       noalloc_init_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, d_Ks, nK, shift, V.WARPS * 32);
       if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
-      setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0]);
+      setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0], 1);
       if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
       chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st, 0);
       if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }

@@ -1,5 +1,5 @@
 /* ap26_cli.c -- the `ap26` command: AP26 KMIN KMAX SHIFT [-compute]
- *                [-device N] [-batch N] [-stop-after N]
+ *                [-device N] [-batch N] [-stop-after N] [-stop-at-word W]
  *
  * Keeps the reference's command-line contract (ibethune/ap26
  * src/common/AP26.cpp:660-1041): resume from AP26-state.{a,b}.txt, search
@@ -14,6 +14,14 @@
  * after N searched K with the checkpoint of the next K written and no hash
  * line, the way a BOINC client stops a task between K; running the command
  * again resumes there.
+ *
+ * Inside a K the command writes the states the reference's CPU build writes
+ * between its 4-word passes (src/cpu/cpuavx2.cpp:858-861): the SOL lines of
+ * shift words 0-3, then the state (K, ITER 4, hash of those words), the
+ * lines of words 4-7, then (K, ITER 8, hash), from the per-word hash sums
+ * the device keeps (ap26_search_k_sol_words).  -stop-at-word W (4 or 8)
+ * ends the process right after the state with ITER W, as a client stopped
+ * there would; running the command again continues K at shift word W.
  */
 #include <stdint.h>
 #include <stdio.h>
@@ -90,14 +98,14 @@ static void write_hash_line(void) {                         /* AP26.cpp:295-357 
 }
 
 int main(int argc, char **argv) {
-  int K, SHIFT, ITER = 0, device = 0, batch = 0, stop_after = 0, searched = 0;
+  int K, SHIFT, ITER = 0, device = 0, batch = 0, stop_after = 0, searched = 0, stop_word = 0;
   printf("AP26 B200 10-shift search version 1.0 (sm_100a, libap26 %d)\n", ap26_version());
   fprintf(stderr, "Command line: ");
   for (int i = 0; i < argc; i++) fprintf(stderr, "%s ", argv[i]);
   fprintf(stderr, "\n");
   if (argc < 4) {
-    printf("Usage: %s KMIN KMAX SHIFT [-compute] [-device N] [-batch N] [-stop-after N]\n",
-           argv[0]);
+    printf("Usage: %s KMIN KMAX SHIFT [-compute] [-device N] [-batch N] [-stop-after N] "
+           "[-stop-at-word W]\n", argv[0]);
     exit(EXIT_FAILURE);
   }
   sscanf(argv[1], "%d", &KMIN);
@@ -108,6 +116,7 @@ int main(int argc, char **argv) {
     else if (!strcmp(argv[i], "-device") && i + 1 < argc) device = atoi(argv[++i]);
     else if (!strcmp(argv[i], "-batch") && i + 1 < argc) batch = atoi(argv[++i]);
     else if (!strcmp(argv[i], "-stop-after") && i + 1 < argc) stop_after = atoi(argv[++i]);
+    else if (!strcmp(argv[i], "-stop-at-word") && i + 1 < argc) stop_word = atoi(argv[++i]);
   }
   if (ap26_read_state("", KMIN, KMAX, SHIFT, &K, &ITER, &result_hash, &last_trickle,
                       &write_state_a_next)) {
@@ -153,7 +162,8 @@ int main(int argc, char **argv) {
   const int cap = 1 << 16;
   ap26_ap *aps = (ap26_ap *)malloc(sizeof(ap26_ap) * cap);
   ap26_sol *sols = (ap26_sol *)malloc(sizeof(ap26_sol) * cap);
-  if (!aps || !sols) die("out of memory");
+  int32_t *sol_word = (int32_t *)malloc(sizeof(int32_t) * cap);
+  if (!aps || !sols || !sol_word) die("out of memory");
   while (K <= KMAX) {
     if (batch > 1 && ITER == 0) {   /* a K resumed mid-way goes through the per-K path */
       /* next group of up to `batch` searchable K */
@@ -182,12 +192,37 @@ int main(int argc, char **argv) {
       checkpoint(SHIFT, K, ITER);
       int n = 0;
       ap26_stats st;
+      int32_t h = result_hash, hash_at[10];
       time_t t0 = time(NULL);
       /* SearchAP26 + ReportSolution of its results, both on the device */
-      rc = ap26_search_k_sol(ctx, K, SHIFT, ITER, &result_hash, sols, cap, &n, &st);
+      rc = ap26_search_k_sol_words(ctx, K, SHIFT, ITER, &h, hash_at, sols, sol_word, cap, &n,
+                                   &st);
       if (rc == AP26_E_INVALID) computation_error();
       if (rc != AP26_OK) die(ap26_strerror(rc));
-      write_sols(sols, n);
+      /* the reference CPU build's pass boundaries: lines of the pass, then
+         the checkpoint with the hash of the words before ITER */
+      int written = 0;
+      for (int it = 4; it < 10; it += 4) {
+        if (it <= ITER) continue;
+        int e = written;
+        while (e < n && sol_word[e] < it) e++;
+        write_sols(sols + written, e - written);
+        written = e;
+        result_hash = hash_at[it - 1];
+        checkpoint(SHIFT, K, it);
+        if (stop_word == it) {
+          if (results_file) fclose(results_file);
+          fprintf(stderr, "Stopped at shift word %d of K %d; resume with the same command.\n",
+                  it, K);
+          free(aps);
+          free(sols);
+          free(sol_word);
+          ap26_destroy(ctx);
+          return EXIT_SUCCESS;
+        }
+      }
+      write_sols(sols + written, n - written);
+      result_hash = h;
       fprintf(stderr, "K %d done in %d sec (%.1f ms device, %lld candidates).\n", K,
               (int)(time(NULL) - t0), st.device_ms, (long long)st.candidates);
       ITER = 0;
@@ -203,6 +238,7 @@ int main(int argc, char **argv) {
     fprintf(stderr, "Stopped after %d K; resume with the same command.\n", searched);
     free(aps);
     free(sols);
+    free(sol_word);
     ap26_destroy(ctx);
     return EXIT_SUCCESS;
   }
@@ -211,6 +247,7 @@ int main(int argc, char **argv) {
   fprintf(stderr, "Workunit complete.\n");
   free(aps);
   free(sols);
+  free(sol_word);
   ap26_destroy(ctx);
   return EXIT_SUCCESS;
 }

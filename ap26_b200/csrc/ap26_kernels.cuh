@@ -46,6 +46,10 @@
 #include <utility>
 #include "ap26_const.cuh"
 
+#ifndef AP26_TAIL_PAIR_LOADS
+#define AP26_TAIL_PAIR_LOADS 0
+#endif
+
 namespace ap26 {
 
 // ---- device data ------------------------------------------------------------
@@ -55,7 +59,7 @@ struct KJob {
   int64_t tile_begin;         // global index of this job's first tile
   int32_t K, shift, item, ntiles;
   int32_t word_begin;         // first shift word reported (the reference's ITER)
-  int32_t pad;
+  int32_t table;              // index of this job's sieve bitstrings in SieveArgs::tables
 };
 
 struct Cand {
@@ -89,7 +93,7 @@ enum : unsigned int {
 struct SieveArgs {
   const KJob *jobs;
   int njobs;
-  const uint32_t *tables;       // [njobs][TABLE_WORDS]
+  const uint32_t *tables;       // [*][TABLE_WORDS], job j's at KJob::table
   DevState *st;
   Cand *cand;
   long long cand_cap;
@@ -238,6 +242,17 @@ __device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w
   return kept;
 }
 
+// Word j of the bitstrings as a single 32-bit load from the pair table.
+// Word j sits both at 32-bit index 2j (pair j, low half) and at 2j-1 (pair
+// j-1, high half); taking 2j for j mod 32 < 16 and 2j-1 otherwise puts any
+// 32 consecutive words in 32 distinct banks.  Tail items of one warp read
+// windows anywhere in a prime's (p + 640)-bit span, up to 35 words: with
+// 64-bit pair loads (16 lanes per phase over up to 35 pairs) they conflict,
+// with these loads only words 32 apart can.
+__device__ __forceinline__ uint32_t word_skewed(const uint32_t *__restrict__ tab, uint32_t j) {
+  return tab[2 * j - ((j >> 4) & 1u)];
+}
+
 // One word of prime P (runtime parameters, identical for all lanes).
 __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
                                               const PrimeParam &P, uint32_t a, uint32_t b,
@@ -246,11 +261,19 @@ __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
   const uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
   const uint32_t pos = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k) + w64;
   const uint32_t w = pos >> 5;
+  const uint32_t sh = pos & 31;
+#if AP26_TAIL_PAIR_LOADS
   const uint2 u = *pair_at(tab, (uint32_t)P.off, w);
   const uint32_t v2 = pair_at(tab, (uint32_t)P.off, w + 2)->x;
-  const uint32_t sh = pos & 31;
   lo &= __funnelshift_r(u.x, u.y, sh);
   hi &= __funnelshift_r(u.y, v2, sh);
+#else
+  const uint32_t j = (uint32_t)P.off + w;
+  const uint32_t v0 = word_skewed(tab, j), v1 = word_skewed(tab, j + 1),
+                 v2 = word_skewed(tab, j + 2);
+  lo &= __funnelshift_r(v0, v1, sh);
+  hi &= __funnelshift_r(v1, v2, sh);
+#endif
 }
 
 // Tail stages g_begin..g_end-1: every queued item advances R primes per pass
@@ -435,7 +458,7 @@ sieve_kernel(SieveArgs A) {
         }
       }
       if (job < 0) break;
-      const uint32_t *src = A.tables + (size_t)job * TABLE_WORDS;
+      const uint32_t *src = A.tables + (size_t)A.jobs[job].table * TABLE_WORDS;
       for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) {
         tab[2 * i] = src[i];
         tab[2 * i + 1] = (i + 1 < TABLE_WORDS) ? src[i + 1] : 0u;
@@ -652,8 +675,16 @@ struct ReportArgs {
   long long n;                       // reports (cap when count is set)
   const KJob *jobs;
   FinRec *fin;
-  unsigned long long *job_hash;      // per-job sum of hash_add (status OK), or null
+  unsigned long long *job_hash;      // per job and shift word: sum of hash_add
+                                     // (status OK), [job * WORDS + w], or null
 };
+
+// Shift word (0..9) of a raw report: its candidate n = n59 + (shift + 64w +
+// b) * MOD with 0 <= n59 < MOD.
+__device__ __forceinline__ int report_word(int64_t n, int shift) {
+  const int t = (int)((uint64_t)n / (uint64_t)MOD) - shift;
+  return min(max(t >> 6, 0), WORDS - 1);
+}
 
 constexpr int REPORT_WARPS = 4;
 enum : uint8_t { TERM_DOM = 1, TERM_P2 = 2, TERM_P9 = 4 };
@@ -767,7 +798,8 @@ __global__ void __launch_bounds__(REPORT_WARPS * 32) report_kernel(ReportArgs A)
       }
       A.fin[r] = out;
       if (A.job_hash && out.status == REP_OK)
-        atomicAdd(&A.job_hash[rec.job], (unsigned long long)out.hash_add);
+        atomicAdd(&A.job_hash[rec.job * WORDS + report_word(rec.n, A.jobs[rec.job].shift)],
+                  (unsigned long long)out.hash_add);
     }
     __syncwarp();
   }

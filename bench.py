@@ -210,26 +210,74 @@ def avx512_companion(k, seconds=8.0):
             "seconds": round(secs, 2)}
 
 
+# ---- parity against the reference's own results ---------------------------------
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def ref_fixture(K, shift):
+    """The reference's raw reports of (K, SHIFT), recorded from its own
+    Search_avx2 (tests/golden/ref_raw), or None where none is recorded."""
+    path = os.path.join(GOLDEN, "ref_raw", f"shift{shift}", f"{K}.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return [tuple(map(int, ln.split())) for ln in f if not ln.startswith("#")]
+
+
+def ref_counts():
+    """(K, SHIFT) -> sieve survivors counted in the reference's own search
+    (tests/golden/ref_counts.json)."""
+    path = os.path.join(GOLDEN, "ref_counts.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        return {(e["K"], e["shift"]): e["survivors"] for e in json.load(f)}
+
+
+def host_hash(A, reports, start=0):
+    """result_hash after the library's host ReportSolution of the reports."""
+    r = A.Reporter(start)
+    r.report_all(reports)
+    return r.hash.value
+
+
+def item_parity(A, items, got_reports, got_hashes):
+    """Items whose every searchable K has a recorded reference fixture: the
+    device reports (in order) and result_hash must equal the reference's
+    reports and their ReportSolution hash."""
+    checked, bad, ks = 0, [], 0
+    for (iid, a, b, sh), reps, h in zip(items, got_reports, got_hashes):
+        exp = []
+        for K in range(a, b + 1):
+            if will_search(K):
+                f = ref_fixture(K, sh)
+                if f is None:
+                    exp = None
+                    break
+                exp += f
+        if exp is None:
+            continue
+        checked += 1
+        ks += sum(will_search(K) for K in range(a, b + 1))
+        if [tuple(r[:3]) for r in reps] != exp or h != host_hash(A, exp):
+            bad.append(iid)
+    return {"items_checked_vs_reference": checked, "k_checked": ks, "items": len(items),
+            "all_items_checked": checked == len(items), "mismatched": bad, "ok": not bad}
+
+
 def parity_check(seen, kmin):
     """Timed-run reports of every K that has a recorded reference raw-report
     fixture (tests/golden/ref_raw/shift0/<K>.txt, the reference's own
     Search_avx2 output) must equal it exactly, in order."""
-    d = os.path.join(ROOT, "tests", "golden", "ref_raw", f"shift{SHIFT}")
     checked, bad = 0, []
     for K in sorted(seen):
-        path = os.path.join(d, f"{K}.txt")
-        if not os.path.exists(path):
+        ref = ref_fixture(K, SHIFT)
+        if ref is None:
             continue
-        ref = []
-        with open(path) as f:
-            for ln in f:
-                if not ln.startswith("#"):
-                    ref.append(tuple(map(int, ln.split())))
         checked += 1
         if seen[K] != ref:
             bad.append(K)
-    k_with_reports = len(seen)
-    return {"k_checked_vs_reference": checked, "k_with_reports": k_with_reports,
+    return {"k_checked_vs_reference": checked, "k_with_reports": len(seen),
             "mismatched": bad, "ok": not bad}
 
 
@@ -261,78 +309,10 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-# ---- extra workloads (not the default line) ----------------------------------------
+# ---- secondary keys of the default line -------------------------------------------
 IMAD_PER_MULMOD = 12   # 32-bit multiply-adds of one 64-bit Montgomery product:
                        # 4 for a*b, 3 for m = lo*n', 4 for hi(m*N), 1 carry
-
-
-def _base_line(metric, value, unit, args, world, workload, extra_cfg):
-    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic (seeded)", "config": dict({"workload": workload}, **extra_cfg)}
-
-
-def workload_sieve(ctx, A, args, world, smem_gbs):
-    """Sieve only: survivor counts of consecutive K at SHIFT=640 (the sieve
-    roofline pair, 1024 K in the full configuration; --k-count sets the size)."""
-    import numpy as np
-    rng = np.random.default_rng(31)
-    k0 = int(rng.integers(1_000_000, 50_000_000 - args.k_count))
-    ks = [k for k in range(k0, k0 + args.k_count)]
-    ctx.sieve_count(ks[:2], 640)     # warm-up
-    counts, st = ctx.sieve_count(ks, 640)
-    cells = st.sieve_cells
-    achieved = cells * CONSULTS_PER_WORD * BYTES_PER_CONSULT / (st.sieve_ms / 1e3) / 1e9
-    line = _base_line("K/s, sieve only (10 shift words)", len(ks) / (st.device_ms / 1e3), "K/s",
-                      args, world, f"sieve survivor counts of {len(ks)} consecutive K from "
-                      f"{k0}, SHIFT=640", {"kmin": k0, "k_count": len(ks), "shift": 640})
-    line["roofline"] = {"bound": "smem", "achieved": achieved, "peak": smem_gbs, "unit": "GB/s",
-                        "frac": achieved / smem_gbs, "kernel": "sieve_kernel"}
-    line["survivors_total"] = int(counts.sum())
-    line["survivors_first"] = [int(c) for c in counts[:4]]
-    return line
-
-
-def workload_prp(ctx, A, args, world, int_tops):
-    """Strong-PRP microbenchmark: 2^prp_log2 odd values in [2^40, 2^63), half
-    primes (selected with the device test, a sample re-checked by the
-    oracle), half odd composites."""
-    import ctypes
-    import numpy as np
-    rng = np.random.default_rng(32)
-    n = 1 << args.prp_log2
-    want = n // 2
-    primes, comps = [], []
-    have_p = have_c = 0
-    while have_p < want or have_c < want:
-        cand = rng.integers(1 << 40, (1 << 63) - 1, 1 << 24, dtype=np.uint64) | np.uint64(1)
-        v, _ = ctx.sprp_batch(cand)
-        p, c = cand[v == 1], cand[v == 0]
-        primes.append(p[:max(0, want - have_p)])
-        comps.append(c[:max(0, want - have_c)])
-        have_p += len(primes[-1])
-        have_c += len(comps[-1])
-    vals = np.concatenate(primes + comps)
-    rng.shuffle(vals)
-    ctx.sprp_batch(vals[:1 << 16])
-    v, st = ctx.sprp_batch(vals)
-    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
-    idx = rng.integers(0, n, 4096)
-    ok = all(L.ao_sprp(ctypes.c_int64(int(vals[i])), ctypes.c_int64(2)) == int(v[i]) for i in idx)
-    squarings = st.late_items
-    mm_s = squarings / (st.device_ms / 1e3)
-    peak = int_tops * 1e12 / IMAD_PER_MULMOD
-    line = _base_line("base-2 SPRP tests/s", n / (st.device_ms / 1e3), "tests/s", args, world,
-                      f"{n} odd values in [2^40, 2^63), half primes", {"values": n})
-    line["mulmod_per_s"] = mm_s
-    line["roofline"] = {"bound": "int", "achieved": mm_s, "peak": peak, "unit": "mulmod/s",
-                        "frac": mm_s / peak, "kernel": "sprp_batch_kernel",
-                        "note": f"peak = measured IMAD rate / {IMAD_PER_MULMOD} multiply-adds "
-                                "per 64-bit Montgomery product; unit = modular squaring"}
-    line["primes"] = int(v.sum())
-    line["parity"] = {"oracle_sample": len(idx), "ok": bool(ok)}
-    return line
+ALG_BYTES_PER_K = N59_PER_K * 10 * CONSULTS_PER_WORD * BYTES_PER_CONSULT
 
 
 def _mixed_items(rng, n, max_len, shifts=(0, 640, 1280)):
@@ -391,84 +371,200 @@ def fixture_pairs():
     return uniq
 
 
-def workload_batched(ctx, A, args, world):
-    """Batched persistent form vs plain one-K-per-launch-sequence form on the
-    same seeded mixed work items (log-uniform lengths 1..64 K, SHIFT from
-    {0, 640, 1280}); --items sets the count (4096 in the full configuration)."""
-    import numpy as np
-    rng = np.random.default_rng(44)
-    items = _mixed_items(rng, args.items, 64)
-    per, res, st = ctx.search_batch(items)
-    bms = st.device_ms
-    nk = sum(r.ks_searched for r in res)
-    t0 = time.perf_counter()
-    pms = 0.0
-    plain = []
-    for (iid, a, b, sh) in items:
-        reps = []
-        for K in range(a, b + 1):
-            if will_search(K):
-                r, s = ctx.search_k(K, sh)
-                pms += s.device_ms
-                reps += r
-        plain.append(reps)
-    same = all(p == q for p, q in zip(per, plain))
-    line = _base_line("K/s, batched persistent form", nk / (bms / 1e3), "K/s", args, world,
-                      f"{len(items)} items, log-uniform 1..64 K, SHIFT in {{0,640,1280}}",
-                      {"items": len(items), "searched_k": nk})
-    line["plain"] = {"value": nk / (pms / 1e3), "unit": "K/s"}
-    line["batched_over_plain"] = (nk / (bms / 1e3)) / (nk / (pms / 1e3))
-    line["parity"] = {"batched_equals_plain_per_item": same}
-    return line
+def _spread(xs):
+    return (max(xs) - min(xs)) / statistics.mean(xs) if len(xs) > 1 else 0.0
 
 
-def workload_serve(ctx, A, args, world):
-    """Continuous-batching service: Poisson arrivals of units (log-uniform
-    1..--serve-max-k K, mixed SHIFT) at 80% of the measured batched
-    capacity; p50/p99 completion latency and sustained K/s."""
+def measure_batched(ctx, A, reps=3, n_items=BATCHED_ITEMS):
+    """The batched persistent form against the plain one-K-per-launch-sequence
+    form on the same seeded mixed items (the first BATCHED_ITEMS of the 4096):
+    each form `reps` times, end to end through the C ABI with host buffers
+    (batched: ap26_search_batch + ap26_report_batch for the SOL lines; plain:
+    ap26_search_k_sol per K, the reference's per-K loop with ReportSolution on
+    the device) and on the device."""
+    items = batched_items(n_items)
+    nk = sum(will_search(K) for _, a, b, _ in items for K in range(a, b + 1))
+    bw, bd, pw, pd = [], [], [], []
+    per = res = None
+    plain_hash = {}
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        per, res, st = ctx.search_batch(items)
+        for reps_i in per:
+            if reps_i:
+                rc, _, _ = ctx.report_batch(reps_i)
+                assert rc == A.OK, rc
+        bw.append(time.perf_counter() - t0)
+        bd.append(st.device_ms / 1e3)
+        t0 = time.perf_counter()
+        dev = 0.0
+        for iid, a, b, sh in items:
+            h = 0
+            for K in range(a, b + 1):
+                if will_search(K):
+                    h, _, s2 = ctx.search_k_sol(K, sh, result_hash=h)
+                    dev += s2.device_ms
+            plain_hash[iid] = h
+        pw.append(time.perf_counter() - t0)
+        pd.append(dev / 1e3)
+    par = item_parity(A, items, per, [r.result_hash for r in res])
+    par["plain_hash_equals_batched"] = all(plain_hash[r.id] == r.result_hash for r in res)
+    par["ok"] = par["ok"] and par["plain_hash_equals_batched"]
+    b_e2e = [nk / t for t in bw]
+    p_e2e = [nk / t for t in pw]
+    return {
+        "workload": f"the first {len(items)} of {BATCHED_FULL_ITEMS} seeded items (seed 44): "
+                    f"log-uniform 1..{BATCHED_MAX_LEN} K, SHIFT in {{0,640,1280}}",
+        "items": len(items), "searched_k": nk, "repeats": reps,
+        "batched": {"e2e_kps": b_e2e, "device_kps": [nk / t for t in bd],
+                    "form": "ap26_search_batch (one CUDA-graph launch per batch) + "
+                            "ap26_report_batch"},
+        "plain": {"e2e_kps": p_e2e, "device_kps": [nk / t for t in pd],
+                  "form": "ap26_search_k_sol per K (search + ReportSolution on the device)"},
+        "e2e_ratio": statistics.mean(b_e2e) / statistics.mean(p_e2e),
+        "device_ratio": statistics.mean(pd) / statistics.mean(bd),
+        "e2e_spread": {"batched": _spread(b_e2e), "plain": _spread(p_e2e)},
+        "parity": par,
+    }
+
+
+def measure_serve(ctx, A, capacity_kps, roofline_kps, n_units=SERVE_UNITS, max_k=SERVE_MAX_K):
+    """Continuous batching: Poisson arrivals of the seeded units at 0.8x the
+    measured batched capacity; units admitted by device memory, two slices
+    queued on the device, each unit's hash and checkpoint kept there."""
     import numpy as np
-    rng = np.random.default_rng(55)
-    units = _mixed_items(rng, args.items, args.serve_max_k)
-    # capacity from one warm batch of 4 K
-    _, _, st = ctx.search_batch([(0, 2_000_003, 2_000_006, 0)])
-    cap_kps = 4 / (st.device_ms / 1e3)
-    mean_k = np.mean([sum(will_search(K) for K in range(a, b + 1)) for _, a, b, _ in units])
-    rate = 0.8 * cap_kps / max(mean_k, 1e-9)          # units per second
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(units)))
+    units = serve_units(n_units, max_k)
+    ks_of = {u[0]: sum(will_search(K) for K in range(u[1], u[2] + 1)) for u in units}
+    mean_k = statistics.mean(ks_of.values())
+    rate = 0.8 * capacity_kps / mean_k                    # units per second
+    arrivals = np.cumsum(np.random.default_rng(56).exponential(1.0 / rate, len(units)))
+    lat, res_of = {}, {}
     t0 = time.perf_counter()
-    nxt, done, lat, total_k = 0, 0, {}, 0
+    nxt, done, total_k = 0, 0, 0
     while done < len(units):
         now = time.perf_counter() - t0
         while nxt < len(units) and arrivals[nxt] <= now:
-            if ctx.serve_submit(*units[nxt]) != 0:
-                break
+            rc = ctx.serve_submit(*units[nxt])
+            assert rc == A.OK, rc
             nxt += 1
         active = ctx.serve_step()
         while True:
             r = ctx.serve_poll()
             if r is None:
                 break
-            res, _aps = r
+            res, aps = r
             lat[res.id] = (time.perf_counter() - t0) - arrivals[res.id]
+            res_of[res.id] = (res, aps)
             total_k += res.ks_searched
             done += 1
-        if active == 0 and nxt < len(units):
-            time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+        now = time.perf_counter() - t0
+        until = arrivals[nxt] - now if nxt < len(units) else 1.0
+        if active == 0:
+            if nxt < len(units):
+                time.sleep(max(0.0, until))
+        else:
+            ctx.serve_wait(max(0.0005, min(until, 1.0)))
     span = time.perf_counter() - t0
     ls = sorted(lat.values())
-    line = _base_line("serve p99 completion latency", float(np.percentile(ls, 99)), "s", args,
-                      world, f"{len(units)} Poisson units, log-uniform 1..{args.serve_max_k} K, "
-                      f"mixed SHIFT, arrivals at 0.8x capacity",
-                      {"units": len(units), "arrival_rate_units_per_s": rate,
-                       "capacity_kps": cap_kps})
-    line["higher_is_better"] = False
-    line["p50_s"] = float(np.percentile(ls, 50))
-    line["p99_s"] = float(np.percentile(ls, 99))
-    line["sustained_kps"] = total_k / span
-    return line
+    # latency at the roofline: the unit's K alone at the sieve's shared-memory roofline
+    frac = sorted(ks_of[i] / roofline_kps / lat[i] for i in lat)
+    par = item_parity(A, units, [res_of[u[0]][1] for u in units],
+                      [res_of[u[0]][0].result_hash for u in units])
+    return {
+        "workload": f"{len(units)} seeded units (seed 55): log-uniform 1..{max_k} K, "
+                    "SHIFT in {0,640,1280}, Poisson arrivals (seed 56) at 0.8x capacity",
+        "max_k": max_k,
+        "units": len(units), "searched_k": total_k, "capacity_kps": capacity_kps,
+        "arrival_rate_units_per_s": rate,
+        "p50_s": float(np.percentile(ls, 50)), "p99_s": float(np.percentile(ls, 99)),
+        "max_s": ls[-1], "sustained_kps": total_k / span,
+        "sustained_frac_of_roofline": total_k / span / roofline_kps,
+        "latency_frac_of_roofline": {"p50": float(np.percentile(frac, 50)),
+                                     "p1": float(np.percentile(frac, 1)),
+                                     "note": "per unit: its K at the sieve roofline alone "
+                                             "/ measured completion latency"},
+        "parity": par,
+    }
+
+
+def measure_sieve_pair(ctx, A, smem_gbs, n=SIEVE_PAIR_K):
+    """Sieve alone: survivor counts of the first SIEVE_PAIR_K of the 1024
+    consecutive K at SHIFT 640; counts of the pinned prefix must equal the
+    reference's own."""
+    ks = sieve_pair_ks(n)
+    counts, st = ctx.sieve_count(ks, SIEVE_PAIR_SHIFT)
+    achieved = st.sieve_cells * CONSULTS_PER_WORD * BYTES_PER_CONSULT / (st.sieve_ms / 1e3) / 1e9
+    pinned = ref_counts()
+    chk = [(k, int(c), pinned[(k, SIEVE_PAIR_SHIFT)]) for k, c in zip(ks, counts)
+           if (k, SIEVE_PAIR_SHIFT) in pinned]
+    return {
+        "workload": f"sieve survivor counts of the first {len(ks)} of {SIEVE_PAIR_FULL} "
+                    f"consecutive K from {SIEVE_PAIR_KMIN}, SHIFT={SIEVE_PAIR_SHIFT}",
+        "k_count": len(ks), "kps": len(ks) / (st.device_ms / 1e3),
+        "raw_kps": len(ks) / (st.device_ms / 1e3),
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_gbs, "unit": "GB/s",
+                     "frac": achieved / smem_gbs, "kernel": "sieve_kernel"},
+        "survivors_total": int(counts.sum()),
+        "parity": {"k_checked_vs_reference": len(chk),
+                   "mismatched": [k for k, c, r in chk if c != r],
+                   "ok": bool(chk) and all(c == r for _, c, r in chk)},
+    }
+
+
+def measure_sprp(ctx, A, int_tops, log2=24):
+    """Strong-PRP microbenchmark: 2^log2 odd values in [2^40, 2^63), half
+    probable primes and half composites as the device test classifies them;
+    verdict parity against the reference's own strong_prp verdicts
+    (tests/golden/sprp_vectors.txt)."""
+    import numpy as np
+    rng = np.random.default_rng(32)
+    n = 1 << log2
+    want = n // 2
+    primes, comps = [], []
+    have_p = have_c = 0
+    while have_p < want or have_c < want:
+        cand = rng.integers(1 << 40, (1 << 63) - 1, 1 << 24, dtype=np.uint64) | np.uint64(1)
+        v, _ = ctx.sprp_batch(cand)
+        p, c = cand[v == 1], cand[v == 0]
+        primes.append(p[:max(0, want - have_p)])
+        comps.append(c[:max(0, want - have_c)])
+        have_p += len(primes[-1])
+        have_c += len(comps[-1])
+    vals = np.concatenate(primes + comps)
+    rng.shuffle(vals)
+    ctx.sprp_batch(vals[:1 << 16])
+    v, st = ctx.sprp_batch(vals)
+    mm_s = st.late_items / (st.device_ms / 1e3)            # modular squarings per second
+    peak = int_tops * 1e12 / IMAD_PER_MULMOD
+    vec = []
+    with open(os.path.join(GOLDEN, "sprp_vectors.txt")) as f:
+        for ln in f:
+            if not ln.startswith("#"):
+                N, a, ver = map(int, ln.split())
+                if a == 2 and N % 2 == 1 and N < (1 << 63):
+                    vec.append((N, ver))
+    vv, _ = ctx.sprp_batch(np.array([x for x, _ in vec], dtype=np.uint64))
+    bad = [N for (N, ver), got in zip(vec, vv) if int(got) != ver]
+    return {
+        "workload": f"{n} odd values in [2^40, 2^63), half primes by the device test (seed 32)",
+        "values": n, "tests_per_s": n / (st.device_ms / 1e3), "mulmod_per_s": mm_s,
+        "roofline": {"bound": "int", "achieved": mm_s, "peak": peak, "unit": "mulmod/s",
+                     "frac": mm_s / peak, "kernel": "sprp_batch_kernel",
+                     "note": f"peak = measured IMAD rate / {IMAD_PER_MULMOD} multiply-adds "
+                             "per 64-bit Montgomery product; unit = modular squaring"},
+        "primes": int(v.sum()),
+        "parity": {"reference_vectors": len(vec), "mismatched": len(bad), "ok": not bad},
+    }
 
 
 # ---- our arm ---------------------------------------------------------------------
+# DRAM bytes of one sieve launch of the default variant (dram__bytes_read.sum +
+# dram__bytes_write.sum from an ncu capture of a 131072-tile launch): the job
+# descriptors, bitstrings and per-CTA flushes, so it scales with launches, not
+# with cells.
+SIEVE_LAUNCH_DRAM_BYTES = None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -478,12 +574,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--workload", default="range",
-                    choices=["range", "sieve", "prp", "batched", "serve"])
-    ap.add_argument("--k-count", type=int, default=64)
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the batched / serve / sieve_pair / sprp keys")
+    # sizes of the secondary keys (defaults: the stated prefixes; the full
+    # configurations are 4096 items, units of 1..256 K and 1024 K)
+    ap.add_argument("--batched-items", type=int, default=BATCHED_ITEMS)
+    ap.add_argument("--serve-units", type=int, default=SERVE_UNITS)
+    ap.add_argument("--serve-max-k", type=int, default=SERVE_MAX_K)
+    ap.add_argument("--sieve-k", type=int, default=SIEVE_PAIR_K)
     ap.add_argument("--prp-log2", type=int, default=24)
-    ap.add_argument("--items", type=int, default=16)
-    ap.add_argument("--serve-max-k", type=int, default=32)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -507,21 +606,7 @@ def main():
         tuned = ctx.autotune(KMIN_SEEDED + 64 * rank if will_search(KMIN_SEEDED + 64 * rank)
                              else KMIN_SEEDED)
     smem_gbs, int_tops = ctx.probe_peaks()
-    if args.workload != "range":
-        fn = {"sieve": lambda: workload_sieve(ctx, A, args, world, smem_gbs),
-              "prp": lambda: workload_prp(ctx, A, args, world, int_tops),
-              "batched": lambda: workload_batched(ctx, A, args, world),
-              "serve": lambda: workload_serve(ctx, A, args, world)}[args.workload]
-        with ClockSampler(local) as clk:
-            line = fn()
-        line["clocks"] = clk.summary()
-        line["autotuned"] = tuned
-        if rank == 0:
-            print(json.dumps(line), flush=True)
-        ctx.close()
-        if world > 1:
-            dist.destroy_process_group()
-        return
+    roofline_kps = smem_gbs * 1e9 / ALG_BYTES_PER_K
     kmin, _ = replicas.rank_range(KMIN_SEEDED, RANGE_K, rank)
     nsteps_range = RANGE_K // STEP_K
 
@@ -530,13 +615,15 @@ def main():
         return [(i, k0, k0 + STEP_K - 1, SHIFT)]
 
     seen = {}
+    item_hash = {}
 
     def run_step(i, sol_lines):
         # the public API a host uses for a workunit: ap26_search_batch (raw
         # reports and the item's result_hash, computed on the device), then
         # ap26_report_batch for the SOL lines (device-side ReportSolution)
         t0 = time.perf_counter()
-        per, res, st = ctx.search_batch(step_items(i))
+        its = step_items(i)
+        per, res, st = ctx.search_batch(its)
         for reps in per:
             if reps:
                 rc, fin, _ = ctx.report_batch(reps)
@@ -549,10 +636,12 @@ def main():
             for k, K, first, _n in reps:
                 local.setdefault(K, []).append((k, K, first))
         seen.update(local)
+        item_hash[its[0][1]] = (res[0].result_hash, its[0][1], its[0][2])
         nk = sum(r.ks_searched for r in res)
         naps = sum(r.n_aps for r in res)
         h2d = KJOB_BYTES * nk + DEVSTATE_BYTES + APREC_BYTES * naps
-        d2h = DEVSTATE_BYTES + 2 * COUNT_BYTES * nk + (APREC_BYTES + FINAL_BYTES) * naps
+        d2h = DEVSTATE_BYTES + (COUNT_BYTES + 10 * COUNT_BYTES) * nk + \
+            (APREC_BYTES + FINAL_BYTES) * naps
         return st, wall, nk, h2d, d2h
 
     for i in range(args.warmup):
@@ -588,43 +677,64 @@ def main():
         barrier()
         wall = time.perf_counter() - t0
     ev_ms = ev0.elapsed_time(ev1)
+    raw_k = STEP_K * args.steps
 
     vec = torch.tensor([tot["dev_ms"], wall, ev_ms, tot["sieve_ms"]], dtype=torch.float64,
                        device="cuda")
-    ks_all = torch.tensor([tot["ks"]], dtype=torch.float64, device="cuda")
+    ks_all = torch.tensor([tot["ks"], raw_k], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(vec, op=dist.ReduceOp.MAX)
         dist.all_reduce(ks_all, op=dist.ReduceOp.SUM)
     dev_ms, wall_max, ev_max, _ = vec.tolist()
-    ks_total = ks_all.item()
+    ks_total, raw_total = ks_all.tolist()
 
-    # plain one-K-per-launch-sequence form on the same K (not part of `value`)
+    # plain one-K-per-launch-sequence form over the rank's 64-K range once
     plain = None
     if not args.no_plain:
         barrier()
-        pms, pk = 0.0, 0
-        for i in range(args.steps):
-            k0 = kmin + STEP_K * (i % nsteps_range)
-            for K in range(k0, k0 + STEP_K):
-                if will_search(K):
-                    _, st = ctx.search_k(K, SHIFT)
-                    pms += st.device_ms
-                    pk += 1
-        pv = torch.tensor([pms], dtype=torch.float64, device="cuda")
+        pms, pk, t0 = 0.0, 0, time.perf_counter()
+        for K in range(kmin, kmin + RANGE_K):
+            if will_search(K):
+                _, _, st = ctx.search_k_sol(K, SHIFT)
+                pms += st.device_ms
+                pk += 1
+        pwall = time.perf_counter() - t0
+        pv = torch.tensor([pms, pwall], dtype=torch.float64, device="cuda")
+        pkt = torch.tensor([pk], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(pv, op=dist.ReduceOp.MAX)
-        plain = {"value": ks_total / (pv.item() / 1000.0), "unit": "K/s",
-                 "form": "ap26_search_k: one K per launch sequence"}
+            dist.all_reduce(pkt, op=dist.ReduceOp.SUM)
+        plain = {"value": pkt.item() / (pv[0].item() / 1000.0), "unit": "K/s",
+                 "e2e": pkt.item() / pv[1].item(), "searched_k": int(pkt.item()),
+                 "form": "ap26_search_k_sol per K over the 64-K range (search + ReportSolution "
+                         "on the device), device time and wall clock"}
+
+    secondary = {}
+    if rank == 0 and world == 1 and not args.no_secondary:
+        with ClockSampler(local) as clk2:
+            secondary["batched"] = measure_batched(ctx, A, n_items=args.batched_items)
+            cap = statistics.mean(secondary["batched"]["batched"]["device_kps"])
+            secondary["serve"] = measure_serve(ctx, A, cap, roofline_kps, args.serve_units,
+                                               args.serve_max_k)
+            secondary["sieve_pair"] = measure_sieve_pair(ctx, A, smem_gbs, args.sieve_k)
+            secondary["sprp"] = measure_sprp(ctx, A, int_tops, args.prp_log2)
+        secondary["clocks"] = clk2.summary()
 
     if rank == 0:
         sieve_launch_ms = tot["sieve_ms"] / max(1, tot["launches"])
         cells_per_launch = tot["cells"] / max(1, tot["launches"])
         alg_bytes = cells_per_launch * CONSULTS_PER_WORD * BYTES_PER_CONSULT
         achieved = alg_bytes / (sieve_launch_ms / 1000.0) / 1e9
-        # DRAM traffic of one sieve launch, scaled by cells from the committed
-        # ncu capture (profiles/sieve_kernel_ncu.md: 69.4 KB read + 2.8 KB
-        # written by an 8385-tile launch of the default variant)
-        traffic = 72.2e3 * (tot["cells"] / max(1, tot["launches"])) / (8385 * 256 * 350)
+        hash_par = {"items": 0, "ok": True}
+        for h, a, b in item_hash.values():
+            exp = []
+            for K in range(a, b + 1):
+                if will_search(K):
+                    f = ref_fixture(K, SHIFT)
+                    exp = None if f is None or exp is None else exp + f
+            if exp is not None:
+                hash_par["items"] += 1
+                hash_par["ok"] = hash_par["ok"] and h == host_hash(A, exp)
         line = {
             "metric": "K/s, 10-shift search", "value": ks_total / (dev_ms / 1000.0),
             "unit": "K/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -634,24 +744,27 @@ def main():
                                    f"rank, SHIFT=0, steps of {STEP_K} K via the batched "
                                    "persistent pipeline",
                        "kmin": KMIN_SEEDED, "k_per_rank": RANGE_K, "shift": SHIFT,
-                       "searched_k": int(ks_total),
+                       "searched_k": int(ks_total), "raw_k": int(raw_total),
                        "parallelism": f"replicas x{world} (disjoint K ranges)",
                        "l2": "working set is a 10 KB table per K in shared memory; no "
                              "HBM-resident inputs to flush",
                        "autotuned": tuned},
+            "raw_kps": raw_total / (dev_ms / 1000.0),
             "e2e": {"value": ks_total / wall_max, "unit": "K/s",
+                    "raw_kps": raw_total / wall_max,
                     "h2d_bytes_per_step": tot["h2d"] // args.steps,
                     "d2h_bytes_per_step": tot["d2h"] // args.steps,
                     "includes": "C-ABI calls (ap26_search_batch + ap26_report_batch), job "
                                 "H2D, report/result D2H, device-side ReportSolution and hash"},
             "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_gbs,
                          "unit": "GB/s", "frac": achieved / smem_gbs,
-                         "traffic": traffic,
+                         "traffic": SIEVE_LAUNCH_DRAM_BYTES,
                          "kernel": "sieve_kernel",
                          "note": "algorithmic bytes = cells x 16.62 consults x 8 B; peak = "
                                  "measured conflict-free LDS.128 bandwidth of this GPU "
                                  "(ap26_probe_peaks); HBM and tensor cores are not on the path",
-                         "launch_ms": sieve_launch_ms, "int_tops_peak": int_tops},
+                         "launch_ms": sieve_launch_ms, "int_tops_peak": int_tops,
+                         "roofline_kps": roofline_kps},
             "gpu_launches": tot["kernels"],
             "torch_event_ms": ev_max,
             "clocks": clk.summary(),
@@ -659,9 +772,17 @@ def main():
         if plain:
             line["plain"] = plain
         line["parity"] = parity_check(seen, kmin)
+        line["parity"]["item_hash"] = hash_par
+        line["parity"]["ok"] = line["parity"]["ok"] and hash_par["ok"]
+        line.update(secondary)
         if world == 1 and not args.no_cpu_baseline:
             ks = [k for k in range(KMIN_SEEDED, KMIN_SEEDED + RANGE_K) if will_search(k)]
-            line["cpu_baseline"] = cpu_baseline_value(ks, 6)
+            cb = cpu_baseline_value(ks, 6)
+            cb["extrapolated"] = ("per-pass time per lattice value from a bounded sample, "
+                                  "times the 10840 lattice values of a pass, plus set-up; "
+                                  "checked once against a whole K (591 s estimated, 614 s "
+                                  "measured on one core)")
+            line["cpu_baseline"] = cb
             comp = avx512_companion(ks[0])
             if comp:
                 line["cpu_avx512"] = comp

@@ -56,20 +56,30 @@ typedef struct {
   int32_t block_threads;  /* sieve CTA size (multiple of 32)                  */
   int32_t late_stage;     /* prime index where items move to the late queue   */
   int32_t chunk_tiles;    /* sieve tiles (one n53 start per CTA thread) per
-                             launch                                           */
-  int32_t use_graphs;     /* 1 = capture per-chunk work in CUDA graphs        */
+                             launch (default 131072, about a quarter of a K;
+                             the autotuner times the sizes the rings hold)    */
+  int32_t use_graphs;     /* 1 (default) = every run (set-up, chunks, chain
+                             walks, ReportSolution, read-backs) is one CUDA
+                             graph launch, captured once per run shape and
+                             cached; -1 = plain stream launches               */
   int32_t profile;        /* 1 = time every sieve launch with CUDA events
-                             (ap26_stats.sieve_ms; disables graph replay)     */
+                             (ap26_stats.sieve_ms; in a graph the events are
+                             event-record nodes)                              */
   int32_t cand_ring_log2; /* each of the two candidate rings holds 2^n
-                             entries (default 23; 12..26).  A chunk whose
-                             survivors overflow it is redone with 4x fewer
-                             tiles per launch (at most six times)             */
-  int64_t mem_budget;     /* bytes of device memory held by admitted serving
-                             units (ap26_serve_submit)                        */
+                             entries of 16 bytes (default 25; 12..27).  A
+                             chunk whose survivors overflow it is redone with
+                             4x fewer tiles per launch (at most six times)    */
+  int64_t mem_budget;     /* serving: device bytes for admitted units' tables
+                             and the fixed serving buffers; 0 = half of the
+                             device memory free at the first admission, at
+                             most 8 GiB (see ap26_serve_submit)               */
   double wait_timeout_s;  /* limit of each host wait on the device (default
                              3600 s); beyond it the call returns
                              AP26_E_TIMEOUT, and the next call on the context
                              first waits for the abandoned work to finish     */
+  int32_t tail_group;     /* primes a queued shift word advances per pass of
+                             the tail stages                                  */
+  int32_t reserved;
 } ap26_opts;
 
 /* One raw report: AP length k, difference multiplier K, first term, and the
@@ -158,12 +168,13 @@ int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out);
 void ap26_destroy(ap26_ctx *ctx);
 int ap26_get_opts(const ap26_ctx *ctx, ap26_opts *out);
 /* Changes the options of a live context; the sieve variant is re-picked
- * from (dense_primes, warp_queue, block_threads, late_stage), zero fields
- * keep their current values.  AP26_E_ARG if no compiled variant matches. */
+ * from (dense_primes, warp_queue, block_threads, late_stage, tail_group),
+ * zero fields keep their current values.  AP26_E_ARG if no compiled variant
+ * matches, or while serving slices are queued. */
 int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts);
 /* The compiled sieve variants (autotuner search space): fills up to cap
- * entries (dense_primes, warp_queue, block_threads, late_stage) and returns
- * the total count. */
+ * entries (dense_primes, warp_queue, block_threads, late_stage, tail_group)
+ * and returns the total count. */
 int ap26_list_variants(ap26_opts *out, int cap);
 
 /* ---- the per-K search (plain GPU form) -----------------------------------
@@ -192,10 +203,25 @@ int ap26_search_k(ap26_ctx *ctx, int K, int shift, ap26_ap *out, int cap,
 int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter, int32_t *result_hash,
                       ap26_sol *sol, int cap, int *n_sol, ap26_stats *stats);
 
+/* ap26_search_k_sol with progress at shift-word granularity, from per-word
+ * hash sums the device keeps for every K-job: hash_at_word[w] (10 entries,
+ * or NULL) is the value *result_hash has after ReportSolution of the reports
+ * of shift words iter..w (for w < iter, the value passed in), and
+ * sol_word[i] (cap entries, or NULL) is the shift word of the report SOL line
+ * i came from.  The reference's CPU build checkpoints between its 4-word
+ * passes (src/cpu/cpuavx2.cpp:858-861, write_state at AP26.cpp:360-390)
+ * with ITER 4 and 8 and the hash of the words before: those states are
+ * (K, 4, hash_at_word[3]) and (K, 8, hash_at_word[7]), and the SOL lines
+ * written by then are the ones with sol_word < ITER, a prefix of sol. */
+int ap26_search_k_sol_words(ap26_ctx *ctx, int K, int shift, int iter, int32_t *result_hash,
+                            int32_t *hash_at_word, ap26_sol *sol, int32_t *sol_word, int cap,
+                            int *n_sol, ap26_stats *stats);
+
 /* ---- batched persistent form ----------------------------------------------
  * All searchable K of all items in one persistent work-stealing pipeline:
  * sieve tiles of every item share launches, survivors of every K share PRP
- * batches.  Reports are grouped per item (res[i].first_ap, res[i].n_aps),
+ * batches, and the whole run (set-up, chunks, chain walks, ReportSolution,
+ * read-backs) is one CUDA-graph launch (ap26_opts.use_graphs).  Reports are grouped per item (res[i].first_ap, res[i].n_aps),
  * inside an item by K ascending, inside a K in AVX2 order.  No counterpart
  * in the reference: it replaces the per-K loop of AP26.cpp:957-982 when many
  * workunits run in one process. */
@@ -204,15 +230,46 @@ int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
                       ap26_item_result *res, ap26_stats *stats);
 
 /* ---- serving: continuous batching ------------------------------------------
- * Units are admitted while the device-memory budget allows (AP26_E_NOMEM
- * otherwise); every ap26_serve_step runs one slice of sieve tiles drawn from
- * all admitted units, so units submitted while others are on the GPU join the
- * next slice.  Finished units are returned by ap26_serve_poll.  No
- * counterpart in the reference (BOINC hands out one workunit per process). */
+ * No counterpart in the reference (BOINC hands out one workunit per
+ * process).  A unit is every searchable K of an item.
+ *
+ * ap26_serve_submit admits a unit while device memory allows, else returns
+ * AP26_E_NOMEM: the unit holds one sieve table (10,272 bytes) per K on the
+ * device from admission to completion, in a pool sized from
+ * ap26_opts.mem_budget at the first admission, together with its checkpoint
+ * slot (at most 1024 units at once).  Admission enqueues the unit's tables
+ * and never waits for work already on the device.
+ *
+ * ap26_serve_step does not block: it takes in every finished slice and keeps
+ * two slices queued on the device while admitted units have K left.  A slice
+ * is up to 4 K-jobs drawn round-robin from the admitted units (each unit's K
+ * in ascending order).  Units submitted while slices run join the next
+ * slice that is built.  *active_units = admitted, unfinished units.
+ * ap26_serve_wait blocks until the oldest queued slice has finished (or
+ * max_wait_s passes: AP26_E_TIMEOUT, nothing lost).
+ * ap26_serve_poll returns 1 and one finished unit (raw reports in the
+ * reference's AVX2 order per K, result_hash computed on the device), or 0.
+ *
+ * Each unit keeps its running ReportSolution hash, survivor count and
+ * checkpoint on the device; every slice reads its units' slots back in
+ * stream order.  ap26_serve_checkpoint returns that checkpoint in the fields
+ * of the reference's state file (ap26_write_state): every K below *K has
+ * been searched (K from shift word *ITER on) and *result_hash is the
+ * reference's result_hash at that point.  ap26_serve_submit_from admits a
+ * unit that resumes from such a state; its result_hash then ends where the
+ * uninterrupted unit's does, and its reports are those of the rest. */
 int ap26_serve_submit(ap26_ctx *ctx, const ap26_item *item);
+int ap26_serve_submit_from(ap26_ctx *ctx, const ap26_item *item, int K, int ITER,
+                           int32_t result_hash);
 int ap26_serve_step(ap26_ctx *ctx, int *active_units);
+int ap26_serve_wait(ap26_ctx *ctx, double max_wait_s);
 int ap26_serve_poll(ap26_ctx *ctx, ap26_item_result *res, ap26_ap *aps,
                     int64_t ap_cap, int64_t *n_aps);
+int ap26_serve_checkpoint(ap26_ctx *ctx, int64_t id, int *kmin, int *kmax, int *shift,
+                          int *K, int *ITER, int32_t *result_hash);
+/* Device bytes the serving pool accounts for: held now (fixed buffers plus
+ * admitted units' tables) and its size. */
+int ap26_serve_memory(const ap26_ctx *ctx, int64_t *in_use, int64_t *budget);
 
 /* ---- kernel-level entry points (parity and roofline measurements) -------- */
 /* Sieve only, over n53 starts [q_begin, q_end) of K (0 <= q < 137375320):
@@ -276,8 +333,11 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
 int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
                              int64_t *d_counts, void *stream);
 
-/* Picks dense_primes / warp_queue / block_threads / chunk_tiles by timing
- * candidates on a fixed K sample, and stores them in the context. */
+/* Picks the sieve variant (dense_primes / warp_queue / block_threads /
+ * late_stage) by timing every compiled one on 1/64 of K's lattice, then
+ * chunk_tiles by timing the whole pipeline over K at each chunk size the
+ * candidate rings hold, and stores them in the context.  K must be
+ * searchable; not while serving slices are queued (AP26_E_ARG). */
 int ap26_autotune(ap26_ctx *ctx, int K, int shift, ap26_opts *chosen);
 
 /* Measured device peaks for the roofline: conflict-free shared-memory load

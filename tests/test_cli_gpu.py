@@ -131,3 +131,51 @@ def test_cli_whole_64k_workunit_matches_reference(tmp_path, oracle):
     expected = sol.value.decode() + hexb.value.decode() + "\n"
     run_cli(tmp_path, kmin, kmax, 0, "-batch", 16)
     assert (tmp_path / "SOL-AP26.txt").read_text() == expected
+
+
+def _ref_states():
+    """(K, ITER) -> result_hash of the states the reference CLI wrote while
+    searching the golden K (tests/golden/ref_states.txt)."""
+    out = {}
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ref_states.txt")) as f:
+        for ln in f:
+            if not ln.startswith("#"):
+                kmin, kmax, shift, K, it, h = map(int, ln.split())
+                out[(kmin, K, it)] = h
+    return out
+
+
+def _newest_state(d, kmin, kmax, shift):
+    import ctypes
+    K, IT, h, tr, nxt = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int32(), ctypes.c_double(),
+                         ctypes.c_int())
+    ok = A.lib.ap26_read_state(str(d).encode(), kmin, kmax, shift, ctypes.byref(K),
+                               ctypes.byref(IT), ctypes.byref(h), ctypes.byref(tr),
+                               ctypes.byref(nxt))
+    assert ok == 1
+    return K.value, IT.value, h.value
+
+
+@pytest.mark.parametrize("K", (366384, 44121555, 47715109))
+def test_cli_writes_the_reference_per_pass_states(tmp_path, K):
+    """Inside a K the command writes the states the reference CPU build
+    writes between its 4-word passes (src/cpu/cpuavx2.cpp:858-861).  Stopped
+    right after the ITER 4 state and again after the ITER 8 state, the newest
+    state equals the reference's (tests/golden/ref_states.txt), the SOL file
+    holds a prefix of the golden lines, and the run resumed from there ends
+    with the golden SOL file and the reference's final state."""
+    st = _ref_states()
+    golden = golden_sol(K).splitlines()
+    p = run_cli(tmp_path, K, K, 0, "-stop-at-word", 4)
+    assert "Checkpoint: KMIN:%d KMAX:%d SHIFT:0 K:%d ITER:4" % (K, K, K) in p.stdout
+    assert _newest_state(tmp_path, K, K, 0) == (K, 4, st[(K, K, 4)])
+    sol = (tmp_path / "SOL-AP26.txt")
+    part = sol.read_text().splitlines() if sol.exists() else []
+    assert part == golden[:len(part)]
+    run_cli(tmp_path, K, K, 0, "-stop-at-word", 8)
+    assert _newest_state(tmp_path, K, K, 0) == (K, 8, st[(K, K, 8)])
+    part2 = sol.read_text().splitlines() if sol.exists() else []
+    assert part2 == golden[:len(part2)] and len(part2) >= len(part)
+    run_cli(tmp_path, K, K, 0)
+    assert sol.read_text() == golden_sol(K)
+    assert _newest_state(tmp_path, K, K, 0) == (K + 1, 0, st[(K, K + 1, 0)])

@@ -209,3 +209,28 @@ def test_search_k_sol_continues_reference_mid_k_checkpoints(ctx, K):
         assert sols == sols_all[len(sols_all) - len(sols):], (K, it)
     with pytest.raises(A.AP26Error):
         ctx.search_k_sol(K, 0, iter=10)
+
+
+@pytest.mark.parametrize("K", GOLDEN_KS)
+def test_search_k_sol_words_gives_the_reference_pass_hashes(ctx, K):
+    """Per-word hash sums kept on the device: the hash after shift words 0-3
+    and 0-7 equals the result_hash of the reference CPU build's ITER 4 and 8
+    checkpoints (tests/golden/ref_states.txt), the last one the final hash;
+    SOL lines come grouped by 4-word pass."""
+    st = {}
+    with open(os.path.join(GOLDEN, "ref_states.txt")) as f:
+        for ln in f:
+            if not ln.startswith("#"):
+                kmin, kmax, shift, KK, it, h = map(int, ln.split())
+                st[(kmin, KK, it)] = h
+    h, sols, words, at, _ = ctx.search_k_sol_words(K, 0)
+    assert at[3] == st[(K, K, 4)]
+    assert at[7] == st[(K, K, 8)]
+    assert at[9] == h == st[(K, K + 1, 0)]
+    passes = [min(w // 4, 2) for w in words]
+    assert passes == sorted(passes)
+    text = "".join(f"{a} {b} {c}\n" for a, b, c in sols) + A.hash_hex(K, K, h) + "\n"
+    assert text == golden_sol(K)
+    # continuing from the ITER 4 state gives the same later words
+    h4, _, _, at4, _ = ctx.search_k_sol_words(K, 0, result_hash=st[(K, K, 4)], iter=4)
+    assert at4[3] == st[(K, K, 4)] and at4[7] == st[(K, K, 8)] and h4 == h
