@@ -92,6 +92,7 @@ __global__ void chunk_begin_kernel(DevState *st, int ring) {
   unsigned long long e = st->chunk_begin + st->chunk_size;
   st->tile_end = e < st->total_tiles ? e : st->total_tiles;
   st->cand_count[ring] = 0;
+  st->chain_next[ring] = 0;
 }
 
 __global__ void chunk_end_kernel(DevState *st, long long cand_cap, int ring) {
@@ -199,8 +200,10 @@ static SieveArgs sieve_args(const KJob *jobs, int njobs, const uint32_t *tables,
 }
 
 static ChainArgs chain_args(const KJob *jobs, DevState *st, const Cand *cand, long long cand_cap,
-                            APRec *aps, long long ap_cap, const unsigned long long *cand_count) {
+                            APRec *aps, long long ap_cap, const unsigned long long *cand_count,
+                            unsigned long long *chain_next) {
   ChainArgs a;
+  a.chain_next = chain_next;
   a.jobs = jobs;
   a.st = st;
   a.cand = cand;
@@ -785,7 +788,7 @@ static cudaError_t emit_run(ap26_ctx *ctx, JobSet &S, const uint32_t *tables, in
     sa[r] = sieve_args(S.d_jobs, njobs, tables, S.d_st, ctx->d_cand[r], ctx->cand_cap,
                        S.d_job_counts, S.count_only ? 1 : 0, &S.d_st->cand_count[r]);
     ca[r] = chain_args(S.d_jobs, S.d_st, ctx->d_cand[r], ctx->cand_cap, S.d_aps, S.ap_cap,
-                       &S.d_st->cand_count[r]);
+                       &S.d_st->cand_count[r], &S.d_st->chain_next[r]);
   }
   const unsigned flag = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
   for (unsigned long long c = 0; c < S.nchunks; c++) {

@@ -79,6 +79,7 @@ struct DevState {
   unsigned long long tile_next, tile_end;      // current chunk window
   unsigned long long chunk_begin, chunk_size, total_tiles;
   unsigned long long cand_count[2];            // per chunk, per candidate ring
+  unsigned long long chain_next[2];            // chain walk's next candidate, per ring
   unsigned long long ap_count, prp_tests, cand_total, late_items;  // per run
   unsigned int err_flags;
   unsigned int pad;
@@ -110,6 +111,7 @@ struct ChainArgs {
   APRec *aps;
   long long ap_cap;
   const unsigned long long *cand_count;
+  unsigned long long *chain_next;   // DevState::chain_next[ring], zero at the chunk's start
 };
 
 // A tile is one n53 start per thread of a sieve CTA: WARPS * 32 starts.
@@ -242,18 +244,17 @@ __device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w
   return kept;
 }
 
-// Word j of the bitstrings as a single 32-bit load from the pair table.
-// Word j sits both at 32-bit index 2j (pair j, low half) and at 2j-1 (pair
-// j-1, high half); taking 2j for j mod 32 < 16 and 2j-1 otherwise puts any
-// 32 consecutive words in 32 distinct banks.  Tail items of one warp read
-// windows anywhere in a prime's (p + 640)-bit span, up to 35 words: with
-// 64-bit pair loads (16 lanes per phase over up to 35 pairs) they conflict,
-// with these loads only words 32 apart can.
-__device__ __forceinline__ uint32_t word_skewed(const uint32_t *__restrict__ tab, uint32_t j) {
-  return tab[2 * j - ((j >> 4) & 1u)];
-}
-
-// One word of prime P (runtime parameters, identical for all lanes).
+// One word of prime P (runtime parameters, identical for all lanes): the 64
+// bits of the window at pos..pos+63, i.e. words j, j+1, j+2 (j = pos / 32)
+// funnel-shifted by pos mod 32.
+// The pair table holds word j both at 32-bit index 2j (pair j, low half) and
+// at 2j-1 (pair j-1, high half).  Reading the three words at B, B+2, B+4
+// with B = 2j - (bit 4 of j) maps any 32 consecutive j to 32 distinct banks
+// (B mod 32 runs over the even banks for j mod 32 < 16 and over the odd ones
+// above), so the lanes of a warp, whose windows lie anywhere in the prime's
+// (p + 640)-bit span of up to 35 words, conflict only for words 32 apart;
+// 64-bit pair loads (16 lanes per phase over up to 35 pairs) conflict far
+// more often.
 __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
                                               const PrimeParam &P, uint32_t a, uint32_t b,
                                               uint32_t c, uint32_t w64, uint32_t &lo,
@@ -269,8 +270,8 @@ __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
   hi &= __funnelshift_r(u.y, v2, sh);
 #else
   const uint32_t j = (uint32_t)P.off + w;
-  const uint32_t v0 = word_skewed(tab, j), v1 = word_skewed(tab, j + 1),
-                 v2 = word_skewed(tab, j + 2);
+  const uint32_t *t = tab + (2 * j - ((j >> 4) & 1u));
+  const uint32_t v0 = t[0], v1 = t[2], v2 = t[4];
   lo &= __funnelshift_r(v0, v1, sh);
   hi &= __funnelshift_r(v1, v2, sh);
 #endif
@@ -585,37 +586,89 @@ __device__ __forceinline__ bool prp_term(DevState *st, int64_t m, unsigned &test
 }
 
 // ---- chain walk: checkn.cl:128-206 / cpuavx2.cpp:532-552 ------------------------
+// For each candidate n (a sieve survivor), with S = K * 23#:
+//   k = 0; m = n + 5S; while (PRP(m)) { k++; m += S; }
+//   if (k >= 10) { m = n + 4S; while (m > 0 && PRP(m)) { k++; m -= S; } }
+//   if (k >= 10) report (k, first = m + S)
+// Walked as a stream of single SPRP tests: each lane holds one chain, runs
+// one test per step, and when its chain ends takes the next candidate of
+// the warp's claimed batch (32 at a time from DevState::chain_next).  A warp
+// that gave each thread a whole chain would run as many tests as its
+// longest chain (about 3.7 for 32 chains) for a mean of about 1.4.
+__device__ __forceinline__ void emit_chain(const ChainArgs &A, int k, int job, int64_t first,
+                                           int64_t n) {
+  unsigned long long j = atomicAdd(&A.st->ap_count, 1ull);
+  if ((long long)j < A.ap_cap) {
+    A.aps[j].k = k;
+    A.aps[j].job = job;
+    A.aps[j].first = first;
+    A.aps[j].n = n;
+  } else {
+    atomicOr(&A.st->err_flags, ERR_AP_OVERFLOW);
+  }
+}
+
 __global__ void chain_kernel(ChainArgs A) {
   const unsigned long long n_c = min(*A.cand_count, (unsigned long long)A.cand_cap);
+  const int lane = threadIdx.x & 31;
   unsigned tests = 0, sq = 0;
-  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_c;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    const Cand cd = A.cand[i];
-    const int64_t S = A.jobs[cd.job].STEP;
-    const int64_t n = cd.n;
-    int k = 0;
-    int64_t m = n + S * 5;
-    while (prp_term(A.st, m, tests, sq)) { k++; m += S; }
-    if (k >= 10) {
-      m = n + S * 4;
-      while (m > 0 && prp_term(A.st, m, tests, sq)) { k++; m -= S; }
+  bool active = false, bwd = false;
+  int64_t n = 0, m = 0, S = 0;
+  int k = 0, job = 0;
+  unsigned long long base = 0;
+  int left = 0;                 // unclaimed-by-lane candidates of the warp's batch
+  bool exhausted = false;
+  for (;;) {
+    // refill: idle lanes take the next candidates of the warp's batch
+    for (;;) {
+      const unsigned idle = __ballot_sync(FULL, !active);
+      if (!idle || exhausted) break;
+      if (left == 0) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(A.chain_next, 32ull);
+        b = __shfl_sync(FULL, b, 0);
+        base = b;
+        left = b < n_c ? (int)min(32ull, n_c - b) : 0;
+        if (left == 0) {
+          exhausted = true;
+          break;
+        }
+      }
+      const int rank = __popc(idle & ((1u << lane) - 1u));
+      const int take = min(__popc(idle), left);
+      if (!active && rank < take) {
+        const Cand cd = A.cand[base + (32 - left) + rank];
+        n = cd.n;
+        job = cd.job;
+        S = A.jobs[job].STEP;
+        m = n + S * 5;
+        k = 0;
+        bwd = false;
+        active = true;
+      }
+      left -= take;
     }
-    if (k >= 10) {
-      unsigned long long j = atomicAdd(&A.st->ap_count, 1ull);
-      if ((long long)j < A.ap_cap) {
-        A.aps[j].k = k;
-        A.aps[j].job = cd.job;
-        A.aps[j].first = m + S;
-        A.aps[j].n = n;
+    if (!__any_sync(FULL, active)) break;
+    if (active) {
+      if (bwd && m <= 0) {          // the backward walk stops below zero, untested
+        emit_chain(A, k, job, m + S, n);
+        active = false;
+      } else if (prp_term(A.st, m, tests, sq)) {
+        k++;
+        m = bwd ? m - S : m + S;
+      } else if (!bwd && k >= 10) {
+        bwd = true;
+        m = n + S * 4;
       } else {
-        atomicOr(&A.st->err_flags, ERR_AP_OVERFLOW);
+        if (k >= 10) emit_chain(A, k, job, m + S, n);
+        active = false;
       }
     }
   }
   // warp-aggregated test counter
   unsigned v = tests;
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&A.st->prp_tests, (unsigned long long)v);
+  if (lane == 0 && v) atomicAdd(&A.st->prp_tests, (unsigned long long)v);
 }
 
 // ---- ReportSolution on the device: AP26.cpp:484-602 ------------------------------
