@@ -191,14 +191,16 @@ def recorded_reference_ks():
 def test_recorded_reference_ranges(ctx):
     """Every K with a recorded reference raw-report file, at every recorded
     SHIFT (0, and 640 / 1280 / 15360 for seeded K): device reports equal
-    the reference's, in order."""
+    the reference's, in order, and the survivor count equals the one
+    counted in the reference's own search wherever that is recorded."""
     import json
     cases = recorded_reference_ks()
     assert len(cases) >= 3 and len({s for _, s in cases}) >= 1
-    # whole-K survivor counts at nonzero SHIFT (tests/golden/make_shift_counts.py)
-    pinned = {(p["K"], p["shift"]): p["candidates"]
-              for p in json.load(open(os.path.join(GOLDEN, "shift_counts.json")))}
-    assert len(pinned) >= 6
+    # whole-K survivor counts counted in the reference's own search
+    # (tests/golden/ref_counts.json, tests/golden/make_golden.py)
+    pinned = {(p["K"], p["shift"]): p["survivors"]
+              for p in json.load(open(os.path.join(GOLDEN, "ref_counts.json")))}
+    assert len({s for _, s in pinned}) >= 3
     for K, shift in cases:
         aps, st = ctx.search_k(K, shift)
         assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(K, shift), (K, shift)

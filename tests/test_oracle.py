@@ -156,3 +156,19 @@ def test_oracle_n43_count_and_setup(oracle):
     s = (ctypes.c_int64 * 9)()
     oracle.ao_setup(366384, s)
     assert s[0] == 366384 * 223092870
+
+
+def test_reference_survivor_counts_are_consistent():
+    """tests/golden/ref_counts.json holds survivor counts counted in the
+    reference's own search: K=366384 at SHIFT 0 is its known answer
+    (src/opencl/AP26.h:343), and every entry's report count equals its
+    recorded raw-report file."""
+    import json
+    import os
+    d = json.load(open(os.path.join(GOLDEN, "ref_counts.json")))
+    by = {(e["K"], e["shift"]): e for e in d}
+    assert by[(366384, 0)]["survivors"] == 38838420
+    assert len({s for _, s in by}) >= 3
+    for (K, shift), e in by.items():
+        assert len(ref_raw(K, shift)) == e["reports"], (K, shift)
+        assert 30_000_000 < e["survivors"] < 70_000_000
