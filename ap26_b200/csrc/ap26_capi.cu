@@ -32,41 +32,99 @@ __device__ int kmul_mod(int64_t c, int K, int64_t *out) {
   return 0;
 }
 
-// The sieve bitstrings of one (K, SHIFT), built by all threads of a block:
-//   B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
+// Bit j of prime p's bitstring, B_p[j] = OK_p[((j + SHIFT) * MOD) mod p], with
 // OK_p[r] = 0 iff r = (jj * (STEP mod p)) mod p for some jj in [p-23, p]
-// (MAKE_OK, src/cpu/cpusse2.cpp:32-36; setok.cl:79-81).
+// (MAKE_OK, src/cpu/cpusse2.cpp:32-36; setok.cl:79-81).  stinv = (STEP mod
+// p)^-1 mod p, or 0 when p divides STEP.
+__device__ __forceinline__ bool bstr_bit(int p, int stinv, int cm, int sh, int j) {
+  const int r = (j + sh) % p * cm % p;
+  if (!stinv) return r != 0;
+  const int tt = r * stinv % p;
+  return tt != 0 && tt < p - 23;
+}
+
+__device__ int step_inv(int K, int p) {     // (K * 23# mod p)^(p-2) mod p, or 0
+  const int st = (int)(((int64_t)(K % p) * (int)(PRIM23 % p)) % p);
+  if (!st) return 0;
+  int e = p - 2, base = st, r = 1;
+  while (e) { if (e & 1) r = r * base % p; base = base * base % p; e >>= 1; }
+  return r;
+}
+
+// The sieve bitstrings of one (K, SHIFT), built by all threads of a block:
+// the pair bitstring (bit j = B_61[j] & B_67[j]) and one bitstring per prime
+// 2..82 at c_params[g].off.
 __device__ void build_table(int K, int shift, uint32_t *tab) {
   for (int t = threadIdx.x; t < TABLE_WORDS; t += blockDim.x) {
-    int g = 0;
-    while (g + 1 < NPRIMES && c_params[g + 1].off <= t) g++;
-    const int p = c_params[g].p;
-    const int st = (int)(((int64_t)(K % p) * (int)(PRIM23 % p)) % p);
-    int stinv = 0;
-    if (st) {  // st^(p-2) mod p
-      int e = p - 2, base = st, r = 1;
-      while (e) { if (e & 1) r = r * base % p; base = base * base % p; e >>= 1; }
-      stinv = r;
-    }
-    const int cm = (int)(MOD % p);
-    const int sh = shift % p;
-    const int j0 = (t - c_params[g].off) * 32;
     uint32_t word = 0;
-    for (int u = 0; u < 32; u++) {
-      const int x = (j0 + u + sh) % p;
-      const int r = x * cm % p;
-      bool bad;
-      if (st == 0) bad = (r == 0);
-      else { const int tt = r * stinv % p; bad = (tt == 0) || (tt >= p - 23); }
-      if (!bad) word |= 1u << u;
+    if (t < PAIR_WORDS) {
+      const int i0 = step_inv(K, 61), i1 = step_inv(K, 67);
+      const int c0 = (int)(MOD % 61), c1 = (int)(MOD % 67);
+      for (int u = 0; u < 32; u++) {
+        const int j = t * 32 + u;
+        if (bstr_bit(61, i0, c0, shift % 61, j) && bstr_bit(67, i1, c1, shift % 67, j))
+          word |= 1u << u;
+      }
+    } else {
+      int g = 2;
+      while (g + 1 < NPRIMES && c_params[g + 1].off <= t) g++;
+      const int p = c_params[g].p;
+      const int stinv = step_inv(K, p), cm = (int)(MOD % p), sh = shift % p;
+      const int j0 = (t - c_params[g].off) * 32;
+      for (int u = 0; u < 32; u++)
+        if (bstr_bit(p, stinv, cm, sh, j0 + u)) word |= 1u << u;
     }
     tab[t] = word;
   }
 }
 
-// Block j: job j.  Thread 0 sets the reference's per-K constants; the block
-// builds the job's bitstrings at KJob::table unless build_tables is 0 (a
-// serving unit builds its tables once, at admission).
+// The sorted lattice order of K (all threads of a 256-thread block): the
+// 12673 n53 starts of an n43 value, index i = j43*667 + j47*29 + j53, by key
+// (j43*d43 + j47*d47 + j53*d53) mod 4087, d = S * MOD^-1 mod 4087 (a
+// counting sort; the order inside one key is the arrival order).
+__device__ void build_order(int K, uint16_t *perm) {
+  __shared__ int hist[PAIR_P];
+  __shared__ int part[256];
+  __shared__ int d[3];
+  if (threadIdx.x == 0) {
+    int64_t S;
+    const int minv = PAIR_PARAM.A;
+    kmul_mod(PRES5, K, &S); d[0] = (int)(S % PAIR_P) * minv % PAIR_P;
+    kmul_mod(PRES6, K, &S); d[1] = (int)(S % PAIR_P) * minv % PAIR_P;
+    kmul_mod(PRES7, K, &S); d[2] = (int)(S % PAIR_P) * minv % PAIR_P;
+  }
+  for (int i = threadIdx.x; i < PAIR_P; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  auto key = [&](int i) {
+    const int j43 = i / 667, j47 = (i - j43 * 667) / 29, j53 = i - j43 * 667 - j47 * 29;
+    return (j43 * d[0] + j47 * d[1] + j53 * d[2]) % PAIR_P;
+  };
+  for (int i = threadIdx.x; i < N53_PER_N43; i += blockDim.x) atomicAdd(&hist[key(i)], 1);
+  __syncthreads();
+  // exclusive prefix of hist: per-thread runs, their sums scanned by thread 0
+  const int per = (PAIR_P + blockDim.x - 1) / blockDim.x;
+  const int lo = min((int)threadIdx.x * per, PAIR_P), hi = min(lo + per, PAIR_P);
+  int sum = 0;
+  for (int i = lo; i < hi; i++) sum += hist[i];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int i = 0; i < (int)blockDim.x; i++) { const int c = part[i]; part[i] = run; run += c; }
+  }
+  __syncthreads();
+  int run = part[threadIdx.x];
+  for (int i = lo; i < hi; i++) { const int c = hist[i]; hist[i] = run; run += c; }
+  __syncthreads();
+  for (int i = threadIdx.x; i < N53_PER_N43; i += blockDim.x)
+    perm[atomicAdd(&hist[key(i)], 1)] = (uint16_t)i;
+  __syncthreads();
+}
+
+// Block j: job j (256 threads).  Thread 0 sets the reference's per-K
+// constants; the block builds the job's bitstrings and lattice order in its
+// block at KJob::table unless build_tables is 0 (a serving unit builds them
+// once, at admission).
 __global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables, int build_tables) {
   const int j = blockIdx.x;
   if (j >= njobs) return;
@@ -83,7 +141,11 @@ __global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables, int b
     kmul_mod(PRES7, K, &J.S53);
     kmul_mod(PRES8, K, &J.S59);
   }
-  if (build_tables) build_table(K, J.shift, tables + (size_t)J.table * TABLE_WORDS);
+  if (build_tables) {
+    uint32_t *blk = tables + (size_t)J.table * JOB_TABLE_WORDS;
+    build_table(K, J.shift, blk);
+    build_order(K, reinterpret_cast<uint16_t *>(blk + TABLE_WORDS));
+  }
 }
 
 // Chunk bookkeeping; `ring` selects the candidate ring this chunk fills.
@@ -323,8 +385,11 @@ static_assert(sizeof(AdmitArgs) <= 4000, "kernel parameters stay below 4 KB");
 
 __global__ void admit_unit_kernel(const AdmitArgs a, UnitState *units, uint32_t *pool) {
   if (a.write_init && blockIdx.x == 0 && threadIdx.x == 0) units[a.slot] = a.init;
-  if ((int)blockIdx.x < a.n)
-    build_table(a.K[blockIdx.x], a.shift, pool + (size_t)a.table[blockIdx.x] * TABLE_WORDS);
+  if ((int)blockIdx.x < a.n) {
+    uint32_t *blk = pool + (size_t)a.table[blockIdx.x] * JOB_TABLE_WORDS;
+    build_table(a.K[blockIdx.x], a.shift, blk);
+    build_order(a.K[blockIdx.x], reinterpret_cast<uint16_t *>(blk + TABLE_WORDS));
+  }
 }
 
 // Device and pinned host buffers of one pipeline run: K-job descriptors and
@@ -545,7 +610,7 @@ static int jobset_ensure(ap26_ctx *ctx, JobSet &S, int njobs) {
     drop_graphs(ctx);   // graphs hold the old buffers' addresses
   }
   CK(cudaMalloc(&S.d_jobs, sizeof(KJob) * cap));
-  if (S.own_tables) CK(cudaMalloc(&S.d_tables, sizeof(uint32_t) * TABLE_WORDS * (size_t)cap));
+  if (S.own_tables) CK(cudaMalloc(&S.d_tables, sizeof(uint32_t) * JOB_TABLE_WORDS * (size_t)cap));
   CK(cudaMalloc(&S.d_job_counts, sizeof(unsigned long long) * cap));
   CK(cudaMalloc(&S.d_job_hash, sizeof(unsigned long long) * WORDS * cap));
   CK(cudaMalloc(&S.d_st, sizeof(DevState)));
@@ -1009,6 +1074,7 @@ static void fill_job(KJob &J, int K, int shift, int item, int64_t q0, int64_t q1
   J.q_begin = q0;
   J.q_end = q1;
   J.word_begin = word_begin;
+  J.flags = JOB_SORTED;
 }
 
 // Runs jobs, retrying with smaller chunks on a candidate-buffer overflow.
@@ -1226,7 +1292,7 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
 // free at that moment, at most 8 GiB), so a unit is admitted only while its
 // tables fit in memory the device really had.
 constexpr int kSliceJobs = 4;          // K-jobs per serving slice
-constexpr int64_t kTableBytes = (int64_t)TABLE_WORDS * 4;
+constexpr int64_t kTableBytes = (int64_t)JOB_TABLE_WORDS * 4;   // bitstrings + lattice order
 
 static int64_t slice_set_bytes() {
   const int64_t jobs = 64;   // jobset_ensure's minimum capacity
@@ -1269,6 +1335,10 @@ static int serve_admit(ap26_ctx *ctx, const ap26_item *item, int K_start, int it
     return AP26_E_DOMAIN;
   if (iter < 0 || iter >= WORDS || h0 < 0 || h0 > kMaxIntV) return AP26_E_ARG;
   if (K_start < item->kmin || K_start > item->kmax + 1) return AP26_E_ARG;
+  for (const auto &v : ctx->units)      // slices map their jobs back to units by id
+    if (v.item.id == item->id) return AP26_E_ARG;
+  for (const auto &v : ctx->finished)
+    if (v.item.id == item->id) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   int rc;
   if ((rc = serve_pool_init(ctx)) != AP26_OK) return rc;
@@ -1543,6 +1613,7 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
   J.ntiles = (int32_t)tiles;
   J.tile_begin = 0;
   J.table = 0;
+  J.flags = 0;   // natural lattice order: [q_begin, q_end) are the reference's positions
   memset(S.h_st, 0, sizeof(DevState));
   S.h_st->chunk_size = (unsigned long long)std::max<int64_t>(1, tiles);
   S.h_st->total_tiles = (unsigned long long)tiles;
@@ -1855,7 +1926,7 @@ struct NoallocScratch {
   DevState st;
   KJob jobs[AP26_NOALLOC_MAX_K];
   unsigned long long counts[AP26_NOALLOC_MAX_K];
-  uint32_t tables[AP26_NOALLOC_MAX_K][TABLE_WORDS];
+  uint32_t tables[AP26_NOALLOC_MAX_K][JOB_TABLE_WORDS];
 };
 static_assert(sizeof(NoallocScratch) == AP26_NOALLOC_SCRATCH_BYTES,
               "the scratch size stated in ap26.h");
@@ -1883,6 +1954,7 @@ __global__ void noalloc_init_kernel(NoallocScratch *s, const int32_t *Ks, int nK
     J.q_end = ok ? N53_PER_K : 0;
     J.ntiles = ok ? (int32_t)ntiles : 0;
     J.table = j;
+    J.flags = JOB_SORTED;
     s_tiles[j] = J.ntiles;
     s->counts[j] = 0;
   }

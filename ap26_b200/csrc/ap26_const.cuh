@@ -40,20 +40,36 @@ constexpr int PRIMES[NPRIMES] = {
     397, 401, 409, 419, 421, 431, 433, 439, 443, 449, 457, 461, 463, 467, 479,
     487, 491, 499, 503, 509, 521, 523, 541};
 
-// Each prime's bitstring covers p + WIN_EXTRA bits: enough for a 640-bit
-// window (plus a 32-bit funnel word) starting anywhere in [0, p), rounded
-// up to an even word count.
+// Each bitstring covers its period + WIN_EXTRA bits: enough for a 640-bit
+// window (plus a 32-bit funnel word) starting anywhere in one period,
+// rounded up to an even word count.  The first two primes share one
+// bitstring of period 61 * 67 (PAIR_P): bit j is B_61[j] & B_67[j], and a
+// lattice value's window in it starts at n59 * MOD^-1 mod PAIR_P, whose
+// residues mod 61 and mod 67 are the two primes' own starts.  Primes 2..82
+// follow, one bitstring each.
 constexpr int WIN_EXTRA = 672;
+constexpr int PAIR_P = 61 * 67;                      // 4087
 constexpr int nwords(int p) { return ((p + WIN_EXTRA + 31) / 32 + 1) & ~1; }
-constexpr int word_offset(int g) {
-  int o = 0;
-  for (int i = 0; i < g; i++) o += nwords(PRIMES[i]);
+constexpr int PAIR_WORDS = nwords(PAIR_P);           // 150
+constexpr int word_offset(int g) {                   // g >= 2
+  int o = PAIR_WORDS;
+  for (int i = 2; i < g; i++) o += nwords(PRIMES[i]);
   return o;
 }
-constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2568 words, 10272 bytes
+constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2670 words, 10680 bytes
+
+// Lattice order.  The 12673 n53 starts of one n43 value (index j43*667 +
+// j47*29 + j53) are visited sorted by their window start in the pair
+// bitstring, (j43*d43 + j47*d47 + j53*d53) mod PAIR_P with d = S * MOD^-1
+// mod PAIR_P; the 32 starts of a warp then lie within a few bits of each
+// other there (12673 starts over 4087 residues, plus at most 3 for the
+// reductions mod MOD), so the pair bitstring's words are read without bank
+// conflicts.  The order is one 16-bit index per start, built with the tables.
+constexpr int PERM_WORDS = (N53_PER_N43 + 1) / 2;   // 6337 words
+constexpr int JOB_TABLE_WORDS = TABLE_WORDS + PERM_WORDS;   // per K-job, 36,068 bytes
 
 constexpr int64_t mod_pos(int64_t a, int64_t m) { return ((a % m) + m) % m; }
-constexpr int inv_mod(int a, int p) {                // a^-1 mod p, p prime
+constexpr int inv_mod(int a, int p) {                // a^-1 mod p, a coprime to p
   int t = 0, nt = 1, r = p, nr = ((a % p) + p) % p;
   while (nr != 0) {
     int q = r / nr, tmp = t - q * nt;
@@ -71,20 +87,29 @@ constexpr int ilog2(int x) { int k = 0; while ((2 << k) <= x) k++; return k; }
 //   M = ceil(2^(32+k) / p) < 2^32,
 // is exact for every x < 2^31 (round-up reciprocal, error x*(M*p-2^(32+k))
 // / (p*2^(32+k)) < 1/p).
+// For the pair bitstring (p = 4087) x < 3 * 2^16 * 4087 < 2^30 and the
+// error bound x / 2^43 < 1/4087 holds the same way.
 struct PrimeParam {
   int p, A, B, C, k, off;
   uint32_t M;
 };
-constexpr PrimeParam make_param(int g) {
-  int p = PRIMES[g];
+constexpr PrimeParam make_param_p(int p, int off) {
   int minv = inv_mod((int)(MOD % p), p);
   int A = minv;
   int B = (int)(((int64_t)65536 % p) * minv % p);
   int C = (int)((((int64_t)1 << 32) % p) * minv % p);
   int k = ilog2(p);
   uint64_t M = ((uint64_t)1 << (32 + k)) / (uint64_t)p + 1;
-  return PrimeParam{p, A, B, C, k, word_offset(g), (uint32_t)M};
+  return PrimeParam{p, A, B, C, k, off, (uint32_t)M};
 }
+// Prime g's own bitstring (g >= 2; primes 0 and 1 only exist in the pair).
+constexpr PrimeParam make_param(int g) {
+  return make_param_p(PRIMES[g], g >= 2 ? word_offset(g) : 0);
+}
+constexpr PrimeParam PAIR_PARAM = make_param_p(PAIR_P, 0);
+// Dense-phase windows: unit 0 is the pair bitstring (primes 0 and 1), unit
+// u >= 1 is prime u + 1.
+constexpr PrimeParam dense_param(int u) { return u == 0 ? PAIR_PARAM : make_param(u + 1); }
 
 // Residue 0 test helpers for the 7..23 filter (sieve.cl:123-142,
 // cpusse2.cpp:563-568).

@@ -59,8 +59,12 @@ struct KJob {
   int64_t tile_begin;         // global index of this job's first tile
   int32_t K, shift, item, ntiles;
   int32_t word_begin;         // first shift word reported (the reference's ITER)
-  int32_t table;              // index of this job's sieve bitstrings in SieveArgs::tables
+  int32_t table;              // index of this job's block in SieveArgs::tables
+  int32_t flags;              // JOB_SORTED: n53 starts in the sorted lattice order
+  int32_t pad;
 };
+
+enum : int32_t { JOB_SORTED = 1 };
 
 struct Cand {
   int64_t n;
@@ -94,7 +98,8 @@ enum : unsigned int {
 struct SieveArgs {
   const KJob *jobs;
   int njobs;
-  const uint32_t *tables;       // [*][TABLE_WORDS], job j's at KJob::table
+  const uint32_t *tables;       // [*][JOB_TABLE_WORDS] (bitstrings, lattice order),
+                                // job j's at KJob::table
   DevState *st;
   Cand *cand;
   long long cand_cap;
@@ -136,13 +141,6 @@ __device__ __forceinline__ int64_t mod_MOD(uint64_t x) {
 }
 
 // ---- sieve pieces -----------------------------------------------------------
-template <int g>
-__device__ __forceinline__ uint32_t window_start(uint32_t a, uint32_t b, uint32_t c) {
-  constexpr PrimeParam P = make_param(g);
-  uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
-  return x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
-}
-
 // The shared table holds the bitstrings as overlapping 64-bit pairs:
 // pair[i] = (word i, word i+1) for every i, so a window starting at any word
 // is a run of aligned 64-bit loads, pair[w], pair[w+2], ...; for a warp the
@@ -152,44 +150,51 @@ __device__ __forceinline__ const uint2 *pair_at(const uint32_t *tab, uint32_t of
   return reinterpret_cast<const uint2 *>(tab) + off + w;
 }
 
-// All 640 bits (20 words) of prime g ANDed into acc: 11 pair loads, 20
+template <int u>
+__device__ __forceinline__ uint32_t unit_start(uint32_t a, uint32_t b, uint32_t c) {
+  constexpr PrimeParam P = dense_param(u);
+  uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
+  return x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
+}
+
+// All 640 bits (20 words) of dense unit u ANDed into acc: 11 pair loads, 20
 // funnel shifts.
-template <int g>
-__device__ __forceinline__ void dense_prime(const uint32_t *__restrict__ tab, uint32_t a,
-                                            uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
-  constexpr PrimeParam P = make_param(g);
-  const uint32_t s = window_start<g>(a, b, c);
+template <int u>
+__device__ __forceinline__ void dense_unit(const uint32_t *__restrict__ tab, uint32_t a,
+                                           uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
+  constexpr PrimeParam P = dense_param(u);
+  const uint32_t s = unit_start<u>(a, b, c);
   const uint2 *t = pair_at(tab, P.off, s >> 5);
   const uint32_t sh = s & 31;
   uint32_t v[22];
 #pragma unroll
   for (int i = 0; i < 11; i++) {
-    const uint2 u = t[2 * i];
-    v[2 * i] = u.x;
-    v[2 * i + 1] = u.y;
+    const uint2 w = t[2 * i];
+    v[2 * i] = w.x;
+    v[2 * i + 1] = w.y;
   }
 #pragma unroll
   for (int i = 0; i < 20; i++) acc[i] &= __funnelshift_r(v[i], v[i + 1], sh);
 }
 
-// Primes g and g+1 together: acc &= window_g & window_{g+1}, one 3-input
+// Units u and u+1 together: acc &= window_u & window_{u+1}, one 3-input
 // LOP3 per word instead of two ANDs.
-template <int g>
-__device__ __forceinline__ void dense_pair(const uint32_t *__restrict__ tab, uint32_t a,
-                                           uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
-  constexpr PrimeParam P = make_param(g), Q = make_param(g + 1);
-  const uint32_t s = window_start<g>(a, b, c), t = window_start<g + 1>(a, b, c);
+template <int u>
+__device__ __forceinline__ void dense_two(const uint32_t *__restrict__ tab, uint32_t a,
+                                          uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
+  constexpr PrimeParam P = dense_param(u), Q = dense_param(u + 1);
+  const uint32_t s = unit_start<u>(a, b, c), t = unit_start<u + 1>(a, b, c);
   const uint2 *tp = pair_at(tab, P.off, s >> 5);
   const uint2 *tq = pair_at(tab, Q.off, t >> 5);
   const uint32_t sp = s & 31, sq = t & 31;
   uint32_t vp[22], vq[22];
 #pragma unroll
   for (int i = 0; i < 11; i++) {
-    const uint2 u = tp[2 * i], v = tq[2 * i];
-    vp[2 * i] = u.x;
-    vp[2 * i + 1] = u.y;
-    vq[2 * i] = v.x;
-    vq[2 * i + 1] = v.y;
+    const uint2 x = tp[2 * i], y = tq[2 * i];
+    vp[2 * i] = x.x;
+    vp[2 * i + 1] = x.y;
+    vq[2 * i] = y.x;
+    vq[2 * i + 1] = y.y;
   }
 #pragma unroll
   for (int i = 0; i < 20; i++)
@@ -197,18 +202,21 @@ __device__ __forceinline__ void dense_pair(const uint32_t *__restrict__ tab, uin
 }
 
 template <int... I>
-__device__ __forceinline__ void dense_pairs(const uint32_t *tab, uint32_t a, uint32_t b,
-                                            uint32_t c, uint32_t (&acc)[20],
-                                            std::integer_sequence<int, I...>) {
-  (dense_pair<2 * I>(tab, a, b, c, acc), ...);
+__device__ __forceinline__ void dense_twos(const uint32_t *tab, uint32_t a, uint32_t b,
+                                           uint32_t c, uint32_t (&acc)[20],
+                                           std::integer_sequence<int, I...>) {
+  (dense_two<2 * I>(tab, a, b, c, acc), ...);
 }
 
-// The first G primes (G even) in pairs.
+// The first G primes (G even): the pair bitstring (primes 0 and 1) and
+// primes 2..G-1, G-1 windows, in twos and one last single.
 template <int G>
 __device__ __forceinline__ void dense_all(const uint32_t *tab, uint32_t a, uint32_t b,
                                           uint32_t c, uint32_t (&acc)[20]) {
-  static_assert(G % 2 == 0, "dense phase works on prime pairs");
-  dense_pairs(tab, a, b, c, acc, std::make_integer_sequence<int, G / 2>{});
+  static_assert(G % 2 == 0 && G >= 4, "dense phase: the pair and an odd number of primes");
+  constexpr int U = G - 1;
+  dense_twos(tab, a, b, c, acc, std::make_integer_sequence<int, U / 2>{});
+  dense_unit<U - 1>(tab, a, b, c, acc);
 }
 
 // Queue item: x = n59 bits 0..31, y = n59 bits 32..47 | w << 16, z/w = mask.
@@ -370,9 +378,12 @@ __device__ __forceinline__ int front_drain(const SieveArgs &A, const uint32_t *t
 // n43 = (n0 + i3*S3 + i5*S5 + i31*S31 + i37*S37 + i41*S41) mod MOD
 // (AP26.h:134) and n53 = n43 + j43*S43 + j47*S47 + j53*S53 mod MOD, the
 // value the reference's nested increments reach (setupn.cl:31-53).
-__device__ __forceinline__ int64_t n53_at(const KJob &J, int64_t q) {
+// With the sorted lattice order (perm != null) the q-th start of an n43
+// value is the perm[q mod 12673]-th of its natural order.
+__device__ __forceinline__ int64_t n53_at(const KJob &J, int64_t q, const uint16_t *perm) {
   int n43i = (int)(q / N53_PER_N43);
   int rem = (int)(q - (int64_t)n43i * N53_PER_N43);
+  if (perm) rem = perm[rem];
   int j43 = rem / 667;
   rem -= j43 * 667;
   int j47 = rem / 29;
@@ -429,6 +440,7 @@ sieve_kernel(SieveArgs A) {
   static_assert(QCAP >= 32 * WORDS, "queue too small for one dense batch");
 
   int cur_job = -1, cur_shift = 0;
+  const uint16_t *cur_perm = nullptr;
   int cnt = 0, lcnt = 0;
   unsigned long long kept_acc = 0, late_acc = 0;
 
@@ -459,7 +471,9 @@ sieve_kernel(SieveArgs A) {
         }
       }
       if (job < 0) break;
-      const uint32_t *src = A.tables + (size_t)A.jobs[job].table * TABLE_WORDS;
+      const uint32_t *src = A.tables + (size_t)A.jobs[job].table * JOB_TABLE_WORDS;
+      cur_perm = (A.jobs[job].flags & JOB_SORTED)
+                     ? reinterpret_cast<const uint16_t *>(src + TABLE_WORDS) : nullptr;
       for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) {
         tab[2 * i] = src[i];
         tab[2 * i + 1] = (i + 1 < TABLE_WORDS) ? src[i + 1] : 0u;
@@ -474,7 +488,7 @@ sieve_kernel(SieveArgs A) {
                        (int64_t)(tile - (unsigned long long)J.tile_begin) * (WARPS * 32) +
                        warp * 32 + lane;
     const bool valid = qi < J.q_end;
-    int64_t n59 = valid ? n53_at(J, qi) : 0;
+    int64_t n59 = valid ? n53_at(J, qi, cur_perm) : 0;
 
     for (int j = 0; j < J59; j++) {
       uint32_t acc[20];

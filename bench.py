@@ -45,7 +45,7 @@ N59_PER_K = 4808136200          # lattice positions per K (10840 n43 x 443555)
 CONSULTS_PER_WORD = 16.62       # oracle: mean table lookups per shift word (canonical order)
 BYTES_PER_CONSULT = 8
 # H2D/D2H payload per K-job and per call (sizes of the C ABI structures)
-KJOB_BYTES, DEVSTATE_BYTES, APREC_BYTES, COUNT_BYTES, FINAL_BYTES = 120, 112, 24, 8, 56
+KJOB_BYTES, DEVSTATE_BYTES, APREC_BYTES, COUNT_BYTES, FINAL_BYTES = 128, 112, 24, 8, 56
 REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 
 

@@ -233,9 +233,11 @@ int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
  * No counterpart in the reference (BOINC hands out one workunit per
  * process).  A unit is every searchable K of an item.
  *
- * ap26_serve_submit admits a unit while device memory allows, else returns
- * AP26_E_NOMEM: the unit holds one sieve table (10,272 bytes) per K on the
- * device from admission to completion, in a pool sized from
+ * ap26_serve_submit admits a unit (its id unique among the units admitted and
+ * not yet polled, AP26_E_ARG otherwise) while device memory allows, else
+ * returns AP26_E_NOMEM: the unit holds one table per K on the device (the
+ * K's sieve bitstrings and lattice order, 36,028 bytes) from admission to
+ * completion, in a pool sized from
  * ap26_opts.mem_budget at the first admission, together with its checkpoint
  * slot (at most 1024 units at once).  Admission enqueues the unit's tables
  * and never waits for work already on the device.
@@ -315,7 +317,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  * valid once that stream reaches this point.
  * - Allocates nothing (no cudaMalloc/cudaFree, no context object): all
  *   scratch -- job descriptors, tables, counters -- lives in one
- *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (665,712 bytes)
+ *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (2,314,608 bytes)
  *   that every GPU loading the library keeps until process exit.  At most
  *   AP26_NOALLOC_MAX_K values of K per call; more returns AP26_E_CAPACITY.
  *   An invalid K costs no sieve time.
@@ -329,7 +331,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  *   calls whose work overlaps on the GPU (other streams, other threads)
  *   race on it and must be serialised by the caller. */
 #define AP26_NOALLOC_MAX_K 64
-#define AP26_NOALLOC_SCRATCH_BYTES 665712
+#define AP26_NOALLOC_SCRATCH_BYTES 2314608
 int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
                              int64_t *d_counts, void *stream);
 

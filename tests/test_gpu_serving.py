@@ -168,14 +168,19 @@ def test_unit_resumed_mid_k_from_a_reference_cpu_checkpoint():
 
 def test_admission_by_device_memory():
     """The pool of tables is sized from mem_budget at the first admission:
-    a unit whose tables do not fit is refused (AP26_E_NOMEM), a small one is
-    admitted, and its bytes are returned when it finishes."""
-    with A.Context(0, mem_budget=12 << 20) as c:
-        assert c.serve_submit(51, 1_000_003, 1_000_003, 0) == 0
-        held, budget = c.serve_memory()
-        assert budget <= 12 << 20
-        room = (budget - held) // 10272
-        assert c.serve_submit(52, 1_000_003, 1_000_003 + 3 * room, 0) == A.E_NOMEM
-        _drain(c)
+    each admitted unit holds its K's tables (the same bytes per K), a unit
+    whose tables do not fit is refused (AP26_E_NOMEM), and a unit's bytes
+    return when it finishes."""
+    with A.Context(0, mem_budget=24 << 20) as c:
+        assert c.serve_submit(51, 1_000_003, 1_000_003, 0) == 0        # 1 searchable K
+        held1, budget = c.serve_memory()
+        assert budget <= 24 << 20
+        assert c.serve_submit(52, 2_000_003, 2_000_004, 0) == 0        # 2 searchable K
         held2, _ = c.serve_memory()
-        assert held2 == held - 10272
+        per_k = (held2 - held1) // 2
+        assert per_k > 10_000 and held2 - held1 == 2 * per_k
+        room = (budget - held2) // per_k
+        assert c.serve_submit(53, 1_000_003, 1_000_003 + 3 * room, 0) == A.E_NOMEM
+        _drain(c)
+        held3, _ = c.serve_memory()
+        assert held3 == held1 - per_k
