@@ -53,12 +53,16 @@ def build(force=False, verbose_ptxas=False):
     if force or not _newer(o, [c] + headers):
         _run(["gcc", "-O2", "-fPIC", "-Wall", "-c", c, "-o", o])
     objs.append(o)
+    # outputs are written under a temporary name and renamed, so a reader
+    # never sees a half-written library or command
     if force or not _newer(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs)
+        os.replace(LIB + ".tmp", LIB)
     cli = os.path.join(CSRC, "ap26_cli.c")
     if force or not _newer(CLI, [cli, LIB]):
-        _run(["gcc", "-O2", "-Wall", "-o", CLI, cli, "-I", os.path.join(ROOT, "include"),
+        _run(["gcc", "-O2", "-Wall", "-o", CLI + ".tmp", cli, "-I", os.path.join(ROOT, "include"),
               "-L", HERE, "-lap26", "-Wl,-rpath,$ORIGIN/.."])
+        os.replace(CLI + ".tmp", CLI)
     return LIB
 
 

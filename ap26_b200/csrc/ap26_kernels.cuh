@@ -27,13 +27,19 @@
 // into ONE window of a p-periodic bitstring:
 //     B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
 //     bit i of the 640-bit mask = B_p[s + i],  s = n59 * MOD^-1 mod p.
-// So each prime needs a (p + 672)-bit string (10 KB for all 83 primes, kept
-// in shared memory) and, per n59, one window offset.  Reading the window is
+// So each prime needs a (p + 672)-bit string (10.7 KB in all, kept in
+// shared memory) and, per n59, one window offset.  Reading the window is
 // conflict-free: all lanes read the same prime's string at word offsets
 // that differ by at most (p-1)/32 < 17, i.e. inside one 32-bank row.
+// Primes 61 and 67 share one string of period 4087 (bit j = B_61[j] &
+// B_67[j], window start n59 * MOD^-1 mod 4087); its windows are read
+// conflict-free because the starts of an n43 value are visited sorted by
+// that window start (ap26_const.cuh), so a warp's 32 starts lie within a
+// few words of each other.
 //
-//   dense phase  the first G primes for all 10 words of every n59 (21 word
-//                loads + 20 funnel shifts per prime)
+//   dense phase  the first G primes for all 10 words of every n59: G-1
+//                windows (the pair, primes 2..G-1), each 21 word loads +
+//                20 funnel shifts
 //   tail         live (n59, word) pairs are compacted into a per-warp shared
 //                queue (ballot/popc) and advanced R primes at a time, all
 //                lanes on the same prime, until stage SL
