@@ -349,8 +349,11 @@ __host__ __device__ inline int32_t hash_fold(int32_t h0, unsigned long long add)
 __global__ void unit_accumulate_kernel(const KJob *jobs, int njobs,
                                        const unsigned long long *job_counts,
                                        const unsigned long long *job_hash, UnitState *units,
-                                       UnitState *snap) {
-  for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
+                                       UnitState *snap, const DevState *st) {
+  // a slice whose buffers overflowed has incomplete sums: it leaves the
+  // units' state as it was (the host fails those units)
+  const bool ok = !(st->err_flags & (ERR_CAND_OVERFLOW | ERR_AP_OVERFLOW));
+  for (int j = threadIdx.x; ok && j < njobs; j += blockDim.x) {
     UnitState &u = units[jobs[j].item];
     unsigned long long h = 0;
     for (int w = 0; w < WORDS; w++) h += job_hash[j * WORDS + w];
@@ -409,6 +412,7 @@ struct JobSet {
   cudaEvent_t t0 = nullptr, done = nullptr;   // around the run, on the main stream
   // shape of the run last enqueued into this set
   int njobs = 0;
+  int chunk_tiles = 0;
   bool count_only = false;
   unsigned long long nchunks = 0, nprof = 0;
   int launches = 0;
@@ -546,7 +550,7 @@ static int default_opts(ap26_opts *o) {
   if (!o->tail_group) o->tail_group = kVariants[0].R;
   if (!o->chunk_tiles) o->chunk_tiles = 131072;
   if (!o->use_graphs) o->use_graphs = 1;
-  if (!o->cand_ring_log2) o->cand_ring_log2 = 25;
+  if (!o->cand_ring_log2) o->cand_ring_log2 = 26;
   if (!(o->wait_timeout_s > 0)) o->wait_timeout_s = 3600.0;
   return 0;
 }
@@ -924,7 +928,8 @@ static cudaError_t capture_run(ap26_ctx *ctx, JobSet &S, const uint32_t *tables,
 // once per run shape and replayed from the cache.
 static int enqueue_jobs(ap26_ctx *ctx, JobSet &S, int njobs, bool count_only, bool overlap,
                         const uint32_t *tables = nullptr, int build_tables = 1,
-                        bool record_done = true) {
+                        bool record_done = true, int chunk_tiles = 0) {
+  if (chunk_tiles <= 0) chunk_tiles = ctx->opts.chunk_tiles;
   int rc;
   if ((rc = jobset_ensure(ctx, S, njobs)) != AP26_OK) return rc;
   if (!tables) tables = S.d_tables;
@@ -941,11 +946,12 @@ static int enqueue_jobs(ap26_ctx *ctx, JobSet &S, int njobs, bool count_only, bo
     tiles += (unsigned long long)J.ntiles;
   }
   memset(S.h_st, 0, sizeof(DevState));
-  S.h_st->chunk_size = (unsigned long long)ctx->opts.chunk_tiles;
+  S.h_st->chunk_size = (unsigned long long)chunk_tiles;
+  S.chunk_tiles = chunk_tiles;
   S.h_st->total_tiles = tiles;
   S.njobs = njobs;
   S.count_only = count_only;
-  S.nchunks = tiles ? (tiles + ctx->opts.chunk_tiles - 1) / ctx->opts.chunk_tiles : 0;
+  S.nchunks = tiles ? (tiles + chunk_tiles - 1) / chunk_tiles : 0;
   const bool two_streams = overlap && !count_only && S.nchunks > 1;
   // sieve launches timed with events: the first kProfChunks chunks at most
   constexpr unsigned long long kProfChunks = 4096;
@@ -956,7 +962,7 @@ static int enqueue_jobs(ap26_ctx *ctx, JobSet &S, int njobs, bool count_only, bo
   bool launched = false;
   if (ctx->opts.use_graphs > 0) {
     const long long key[7] = {(long long)(uintptr_t)&S, ctx->variant, njobs,
-                              (long long)S.nchunks, ctx->opts.chunk_tiles,
+                              (long long)S.nchunks, chunk_tiles,
                               (count_only ? 1 : 0) | (two_streams ? 2 : 0) | (build_tables ? 4 : 0) |
                                   ((long long)S.nprof << 3),
                               (long long)(uintptr_t)tables};
@@ -1023,7 +1029,7 @@ static int collect_run(ap26_ctx *ctx, JobSet &S, cudaStream_t cs, ap26_stats *st
       if (S.nprof < S.nchunks) {
         // only the first nprof chunks were timed; all of them are full
         const int64_t tile_n53 = (int64_t)kVariants[ctx->variant].WARPS * 32;
-        stats->sieve_cells = (int64_t)(S.nprof * (unsigned long long)ctx->opts.chunk_tiles) *
+        stats->sieve_cells = (int64_t)(S.nprof * (unsigned long long)S.chunk_tiles) *
                              tile_n53 * J59 * WORDS;
         stats->sieve_launches = (int32_t)S.nprof;
       }
@@ -1292,6 +1298,20 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
 // free at that moment, at most 8 GiB), so a unit is admitted only while its
 // tables fit in memory the device really had.
 constexpr int kSliceJobs = 4;          // K-jobs per serving slice
+
+// Survivors per tile of 256 n53 starts: about 69 for a K that no sieve
+// prime divides; a sieve prime p dividing K multiplies the density by
+// (p-1)/(p-24) (one bad residue instead of 24), and at most four of them
+// divide a K <= 4e8 (61*67*71*73*79 > 4e8), so at most 5.44 times: about
+// 373.  A serving slice cannot be redone in smaller chunks without finishing
+// after slices queued behind it, so its chunks are sized to this bound.
+constexpr int kMaxSurvivorsPer256Tile = 400;
+
+static int serve_chunk_tiles(const ap26_ctx *ctx) {
+  const int64_t tile_n53 = (int64_t)kVariants[ctx->variant].WARPS * 32;
+  const int64_t bound = ctx->cand_cap * 256 / (kMaxSurvivorsPer256Tile * tile_n53);
+  return (int)std::max<int64_t>(64, std::min<int64_t>(ctx->opts.chunk_tiles, bound));
+}
 constexpr int64_t kTableBytes = (int64_t)JOB_TABLE_WORDS * 4;   // bitstrings + lattice order
 
 static int64_t slice_set_bytes() {
@@ -1465,12 +1485,14 @@ static int launch_slice(ap26_ctx *ctx, Slice &sl) {
     sl.unit_ids.push_back(u->item.id);
   }
   sl.busy = true;
-  sl.rc = enqueue_jobs(ctx, S, (int)picked.size(), false, true, ctx->d_pool, 0, false);
+  sl.rc = enqueue_jobs(ctx, S, (int)picked.size(), false, true, ctx->d_pool, 0, false,
+                       serve_chunk_tiles(ctx));
   if (sl.rc == AP26_OK) {
     // the units' running sums and checkpoints stay on the device; the slice
     // reads back its units' states in stream order, then S.done fires
     unit_accumulate_kernel<<<1, 256, 0, ctx->stream>>>(S.d_jobs, S.njobs, S.d_job_counts,
-                                                       S.d_job_hash, ctx->d_units, sl.d_snap);
+                                                       S.d_job_hash, ctx->d_units, sl.d_snap,
+                                                       S.d_st);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(sl.h_snap, sl.d_snap, sizeof(UnitState) * S.njobs,

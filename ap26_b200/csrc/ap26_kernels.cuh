@@ -52,10 +52,6 @@
 #include <utility>
 #include "ap26_const.cuh"
 
-#ifndef AP26_TAIL_PAIR_LOADS
-#define AP26_TAIL_PAIR_LOADS 0
-#endif
-
 namespace ap26 {
 
 // ---- device data ------------------------------------------------------------
@@ -260,15 +256,7 @@ __device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w
 
 // One word of prime P (runtime parameters, identical for all lanes): the 64
 // bits of the window at pos..pos+63, i.e. words j, j+1, j+2 (j = pos / 32)
-// funnel-shifted by pos mod 32.
-// The pair table holds word j both at 32-bit index 2j (pair j, low half) and
-// at 2j-1 (pair j-1, high half).  Reading the three words at B, B+2, B+4
-// with B = 2j - (bit 4 of j) maps any 32 consecutive j to 32 distinct banks
-// (B mod 32 runs over the even banks for j mod 32 < 16 and over the odd ones
-// above), so the lanes of a warp, whose windows lie anywhere in the prime's
-// (p + 640)-bit span of up to 35 words, conflict only for words 32 apart;
-// 64-bit pair loads (16 lanes per phase over up to 35 pairs) conflict far
-// more often.
+// funnel-shifted by pos mod 32, read as pair j and the low half of pair j+2.
 __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
                                               const PrimeParam &P, uint32_t a, uint32_t b,
                                               uint32_t c, uint32_t w64, uint32_t &lo,
@@ -277,18 +265,10 @@ __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
   const uint32_t pos = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k) + w64;
   const uint32_t w = pos >> 5;
   const uint32_t sh = pos & 31;
-#if AP26_TAIL_PAIR_LOADS
   const uint2 u = *pair_at(tab, (uint32_t)P.off, w);
   const uint32_t v2 = pair_at(tab, (uint32_t)P.off, w + 2)->x;
   lo &= __funnelshift_r(u.x, u.y, sh);
   hi &= __funnelshift_r(u.y, v2, sh);
-#else
-  const uint32_t j = (uint32_t)P.off + w;
-  const uint32_t *t = tab + (2 * j - ((j >> 4) & 1u));
-  const uint32_t v0 = t[0], v1 = t[2], v2 = t[4];
-  lo &= __funnelshift_r(v0, v1, sh);
-  hi &= __funnelshift_r(v1, v2, sh);
-#endif
 }
 
 // Tail stages g_begin..g_end-1: every queued item advances R primes per pass

@@ -66,9 +66,11 @@ typedef struct {
                              (ap26_stats.sieve_ms; in a graph the events are
                              event-record nodes)                              */
   int32_t cand_ring_log2; /* each of the two candidate rings holds 2^n
-                             entries of 16 bytes (default 25; 12..27).  A
+                             entries of 16 bytes (default 26; 12..27).  A
                              chunk whose survivors overflow it is redone with
-                             4x fewer tiles per launch (at most six times)    */
+                             4x fewer tiles per launch (at most six times);
+                             serving slices use chunks small enough for the
+                             densest K                                        */
   int64_t mem_budget;     /* serving: device bytes for admitted units' tables
                              and the fixed serving buffers; 0 = half of the
                              device memory free at the first admission, at

@@ -23,10 +23,13 @@ def run_cli(cwd, *args):
 def test_cli_reproduces_golden_sol_and_final_state(tmp_path):
     run_cli(tmp_path, 366384, 366384, 0)
     assert (tmp_path / "SOL-AP26.txt").read_text() == golden_sol(366384)
-    # checkpoint before the K (state A), final one with K = KMAX+1 (state B)
+    # the states written alternate A/B as the reference's: before the K
+    # (A), after its 4-word passes at ITER 4 (B) and ITER 8 (A), and the
+    # final one with K = KMAX+1 (B); the files keep the last two
+    # (tests/golden/ref_states.txt)
     a = (tmp_path / "AP26-state.a.txt").read_text().split()
     b = (tmp_path / "AP26-state.b.txt").read_text().split()
-    assert a[:6] == ["366384", "366384", "0", "366384", "0", "0"]
+    assert a[:6] == ["366384", "366384", "0", "366384", "8", "72858"]
     assert b[:6] == ["366384", "366384", "0", "366385", "0", "87376"]
 
 

@@ -184,3 +184,29 @@ def test_admission_by_device_memory():
         _drain(c)
         held3, _ = c.serve_memory()
         assert held3 == held1 - per_k
+
+
+def test_densest_k_runs_and_serves_without_overflow():
+    """K = 61*67*71*73 = 21182107 is the densest searchable K below 4e8: the
+    four smallest sieve primes divide K*23#, so each bans one residue
+    instead of 24 and about 5.4 times the usual candidates survive.  The
+    synchronous search redoes an overflowing chunk in smaller ones (here a
+    2^24-entry ring forces it); serving slices size their chunks for this
+    density.  Both give the reference's reports."""
+    K = 21182107
+    ref = ref_raw(K)
+    with A.Context(0, cand_ring_log2=24) as c:
+        aps, st = c.search_k(K, 0)
+        assert st.error_flags & 1                 # redone in smaller chunks
+    assert [(k, KK, f) for k, KK, f, _ in aps] == ref
+    assert st.candidates > 5 * 36_000_000
+    with A.Context(0) as c:
+        assert c.serve_submit(61, K, K, 0) == 0
+        got = _drain(c)
+    res, saps = got[61]
+    assert res.status == 0
+    assert [(k, KK, f) for k, KK, f, _ in saps] == ref
+    assert res.candidates == st.candidates
+    r = A.Reporter()
+    r.report_all(ref)
+    assert res.result_hash == r.hash.value
