@@ -52,21 +52,22 @@ __device__ int step_inv(int K, int p) {     // (K * 23# mod p)^(p-2) mod p, or 0
 }
 
 // The sieve bitstrings of one (K, SHIFT), built by all threads of a block:
-// the pair bitstring (bit j = B_61[j] & B_67[j]) and one bitstring per prime
-// 2..82 at c_params[g].off.
+// the two pair bitstrings (bit j = B_61[j] & B_67[j], then B_71[j] &
+// B_73[j]) and one bitstring per prime 4..82 at c_params[g].off.
 __device__ void build_table(int K, int shift, uint32_t *tab) {
   for (int t = threadIdx.x; t < TABLE_WORDS; t += blockDim.x) {
     uint32_t word = 0;
-    if (t < PAIR_WORDS) {
-      const int i0 = step_inv(K, 61), i1 = step_inv(K, 67);
-      const int c0 = (int)(MOD % 61), c1 = (int)(MOD % 67);
-      for (int u = 0; u < 32; u++) {
-        const int j = t * 32 + u;
-        if (bstr_bit(61, i0, c0, shift % 61, j) && bstr_bit(67, i1, c1, shift % 67, j))
+    if (t < PAIR1_WORDS + PAIR2_WORDS) {
+      const bool first = t < PAIR1_WORDS;
+      const int p = first ? 61 : 71, q = first ? 67 : 73;
+      const int ip = step_inv(K, p), iq = step_inv(K, q);
+      const int cp = (int)(MOD % p), cq = (int)(MOD % q);
+      const int j0 = (first ? t : t - PAIR1_WORDS) * 32;
+      for (int u = 0; u < 32; u++)
+        if (bstr_bit(p, ip, cp, shift % p, j0 + u) && bstr_bit(q, iq, cq, shift % q, j0 + u))
           word |= 1u << u;
-      }
     } else {
-      int g = 2;
+      int g = PAIR_PRIMES;
       while (g + 1 < NPRIMES && c_params[g + 1].off <= t) g++;
       const int p = c_params[g].p;
       const int stinv = step_inv(K, p), cm = (int)(MOD % p), sh = shift % p;
@@ -78,53 +79,60 @@ __device__ void build_table(int K, int shift, uint32_t *tab) {
   }
 }
 
-// The sorted lattice order of K (all threads of a 256-thread block): the
-// 12673 n53 starts of an n43 value, index i = j43*667 + j47*29 + j53, by key
-// (j43*d43 + j47*d47 + j53*d53) mod 4087, d = S * MOD^-1 mod 4087 (a
-// counting sort; the order inside one key is the arrival order).
+// The sorted lattice order of K, built by all threads of a block with
+// ORDER_SMEM bytes of dynamic shared memory: the 12673 n53 starts of an n43
+// value, index i = j43*667 + j47*29 + j53, ordered by (k1 / ORDER_BUCKET,
+// k2, i) with k1 = (j43*d43 + j47*d47 + j53*d53) mod 4087 and k2 the same
+// mod 5183 (d = S * MOD^-1 mod the pair's period): a bitonic sort of
+// 16384 packed keys (18 key bits, 14 index bits; padding sorts last).
+constexpr int ORDER_N = 16384;
+constexpr size_t ORDER_SMEM = sizeof(uint32_t) * ORDER_N;
+static_assert((PAIR1_P / ORDER_BUCKET + 1) * PAIR2_P < (1 << 18), "sort key fits 18 bits");
+
 __device__ void build_order(int K, uint16_t *perm) {
-  __shared__ int hist[PAIR_P];
-  __shared__ int part[256];
-  __shared__ int d[3];
+  extern __shared__ uint32_t sk[];
+  __shared__ int d[6];
   if (threadIdx.x == 0) {
-    int64_t S;
-    const int minv = PAIR_PARAM.A;
-    kmul_mod(PRES5, K, &S); d[0] = (int)(S % PAIR_P) * minv % PAIR_P;
-    kmul_mod(PRES6, K, &S); d[1] = (int)(S % PAIR_P) * minv % PAIR_P;
-    kmul_mod(PRES7, K, &S); d[2] = (int)(S % PAIR_P) * minv % PAIR_P;
-  }
-  for (int i = threadIdx.x; i < PAIR_P; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  auto key = [&](int i) {
-    const int j43 = i / 667, j47 = (i - j43 * 667) / 29, j53 = i - j43 * 667 - j47 * 29;
-    return (j43 * d[0] + j47 * d[1] + j53 * d[2]) % PAIR_P;
-  };
-  for (int i = threadIdx.x; i < N53_PER_N43; i += blockDim.x) atomicAdd(&hist[key(i)], 1);
-  __syncthreads();
-  // exclusive prefix of hist: per-thread runs, their sums scanned by thread 0
-  const int per = (PAIR_P + blockDim.x - 1) / blockDim.x;
-  const int lo = min((int)threadIdx.x * per, PAIR_P), hi = min(lo + per, PAIR_P);
-  int sum = 0;
-  for (int i = lo; i < hi; i++) sum += hist[i];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int i = 0; i < (int)blockDim.x; i++) { const int c = part[i]; part[i] = run; run += c; }
+    int64_t S[3];
+    kmul_mod(PRES5, K, &S[0]);
+    kmul_mod(PRES6, K, &S[1]);
+    kmul_mod(PRES7, K, &S[2]);
+    for (int x = 0; x < 3; x++) {
+      d[x] = (int)(S[x] % PAIR1_P) * PAIR1_PARAM.A % PAIR1_P;
+      d[3 + x] = (int)(S[x] % PAIR2_P) * PAIR2_PARAM.A % PAIR2_P;
+    }
   }
   __syncthreads();
-  int run = part[threadIdx.x];
-  for (int i = lo; i < hi; i++) { const int c = hist[i]; hist[i] = run; run += c; }
+  for (int i = threadIdx.x; i < ORDER_N; i += blockDim.x) {
+    uint32_t v = 0xffffffffu;
+    if (i < N53_PER_N43) {
+      const int j43 = i / 667, j47 = (i - j43 * 667) / 29, j53 = i - j43 * 667 - j47 * 29;
+      const int k1 = (j43 * d[0] + j47 * d[1] + j53 * d[2]) % PAIR1_P;
+      const int k2 = (j43 * d[3] + j47 * d[4] + j53 * d[5]) % PAIR2_P;
+      v = ((uint32_t)((k1 / ORDER_BUCKET) * PAIR2_P + k2) << 14) | (uint32_t)i;
+    }
+    sk[i] = v;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < N53_PER_N43; i += blockDim.x)
-    perm[atomicAdd(&hist[key(i)], 1)] = (uint16_t)i;
+  for (int k = 2; k <= ORDER_N; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < ORDER_N; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const uint32_t a = sk[i], b = sk[ixj];
+          if ((a > b) == ((i & k) == 0)) { sk[i] = b; sk[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < N53_PER_N43; i += blockDim.x) perm[i] = (uint16_t)(sk[i] & 0x3fffu);
   __syncthreads();
 }
 
-// Block j: job j (256 threads).  Thread 0 sets the reference's per-K
-// constants; the block builds the job's bitstrings and lattice order in its
-// block at KJob::table unless build_tables is 0 (a serving unit builds them
-// once, at admission).
+// Block j: job j (256 threads, ORDER_SMEM dynamic shared memory).  Thread 0
+// sets the reference's per-K constants; the block builds the job's
+// bitstrings and lattice order in its block at KJob::table unless
+// build_tables is 0 (a serving unit builds them once, at admission).
 __global__ void setup_jobs_kernel(KJob *jobs, int njobs, uint32_t *tables, int build_tables) {
   const int j = blockIdx.x;
   if (j >= njobs) return;
@@ -687,6 +695,11 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     PrimeParam params[NPRIMES];
     for (int g = 0; g < NPRIMES; g++) params[g] = make_param(g);
     CKC(cudaMemcpyToSymbol(c_params, params, sizeof(params)));
+    // the set-up kernels sort each K's lattice order in 64 KB of shared memory
+    CKC(cudaFuncSetAttribute(setup_jobs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ORDER_SMEM));
+    CKC(cudaFuncSetAttribute(admit_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ORDER_SMEM));
     // buffers
     if (ctx->opts.cand_ring_log2 < 12 || ctx->opts.cand_ring_log2 > 27) {
       rc = AP26_E_ARG;
@@ -847,7 +860,7 @@ static cudaError_t emit_run(ap26_ctx *ctx, JobSet &S, const uint32_t *tables, in
   EM(cudaMemcpyAsync(S.d_st, S.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
   EM(cudaMemsetAsync(S.d_job_counts, 0, sizeof(unsigned long long) * njobs, s));
   EM(cudaMemsetAsync(S.d_job_hash, 0, sizeof(unsigned long long) * WORDS * njobs, s));
-  setup_jobs_kernel<<<njobs, 256, 0, s>>>(S.d_jobs, njobs, const_cast<uint32_t *>(tables),
+  setup_jobs_kernel<<<njobs, 256, ORDER_SMEM, s>>>(S.d_jobs, njobs, const_cast<uint32_t *>(tables),
                                           build_tables);
   EM(cudaGetLastError());
   // ring r: candidate buffer d_cand[r] and its fill count DevState::cand_count[r]
@@ -1403,7 +1416,8 @@ static int serve_admit(ap26_ctx *ctx, const ap26_item *item, int K_start, int it
       a.K[b] = u.ks[i + b];
       a.table[b] = u.tables[i + b];
     }
-    admit_unit_kernel<<<std::max(1, a.n), 256, 0, ctx->stream>>>(a, ctx->d_units, ctx->d_pool);
+    admit_unit_kernel<<<std::max(1, a.n), 256, ORDER_SMEM, ctx->stream>>>(a, ctx->d_units,
+                                                                          ctx->d_pool);
     CK(cudaGetLastError());
     i += (size_t)a.n;
   } while (i < u.ks.size());
@@ -1645,7 +1659,7 @@ extern "C" int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin
   CK(cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(S.d_st, S.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(S.d_job_counts, 0, sizeof(unsigned long long), s));
-  setup_jobs_kernel<<<1, 256, 0, s>>>(S.d_jobs, 1, S.d_tables, 1);
+  setup_jobs_kernel<<<1, 256, ORDER_SMEM, s>>>(S.d_jobs, 1, S.d_tables, 1);
   chunk_begin_kernel<<<1, 1, 0, s>>>(S.d_st, 0);
   const SieveArgs sa = sieve_args(S.d_jobs, 1, S.d_tables, S.d_st, ctx->d_cand[0],
                                   ctx->cand_cap, S.d_job_counts, 0, &S.d_st->cand_count[0]);
@@ -1825,7 +1839,7 @@ extern "C" int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t 
   memset(S.h_st, 0, sizeof(DevState));
   CK(cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(KJob), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(S.d_st, S.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
-  setup_jobs_kernel<<<1, 256, 0, s>>>(S.d_jobs, 1, S.d_tables, 0);
+  setup_jobs_kernel<<<1, 256, ORDER_SMEM, s>>>(S.d_jobs, 1, S.d_tables, 0);
   CK(cudaMemcpyAsync(dn.p, n, sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev0, s));
   chain_explicit_kernel<<<ctx->num_sms * 8, 128, 0, s>>>(S.d_jobs, dn.p, count, dk.p, df.p,
@@ -2024,6 +2038,9 @@ static int noalloc_setup(int device, NoallocDevice **out) {
     for (int g = 0; g < NPRIMES; g++) params[g] = make_param(g);
     if (cudaMemcpyToSymbol(c_triples, trip, sizeof(trip)) != cudaSuccess) return AP26_E_CUDA;
     if (cudaMemcpyToSymbol(c_params, params, sizeof(params)) != cudaSuccess) return AP26_E_CUDA;
+    if (cudaFuncSetAttribute(setup_jobs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ORDER_SMEM) != cudaSuccess)
+      return AP26_E_CUDA;
     const SieveVariant &V = kVariants[0];
     if (cudaFuncSetAttribute(V.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)V.smem()) != cudaSuccess)
@@ -2070,7 +2087,7 @@ extern "C" int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK,
     do {
       noalloc_init_kernel<<<1, AP26_NOALLOC_MAX_K, 0, s>>>(S, d_Ks, nK, shift, V.WARPS * 32);
       if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
-      setup_jobs_kernel<<<nK, 256, 0, s>>>(S->jobs, nK, &S->tables[0][0], 1);
+      setup_jobs_kernel<<<nK, 256, ORDER_SMEM, s>>>(S->jobs, nK, &S->tables[0][0], 1);
       if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }
       chunk_begin_kernel<<<1, 1, 0, s>>>(&S->st, 0);
       if (noalloc_launch_failed()) { rc = AP26_E_CUDA; break; }

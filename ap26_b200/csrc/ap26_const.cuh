@@ -42,31 +42,38 @@ constexpr int PRIMES[NPRIMES] = {
 
 // Each bitstring covers its period + WIN_EXTRA bits: enough for a 640-bit
 // window (plus a 32-bit funnel word) starting anywhere in one period,
-// rounded up to an even word count.  The first two primes share one
-// bitstring of period 61 * 67 (PAIR_P): bit j is B_61[j] & B_67[j], and a
-// lattice value's window in it starts at n59 * MOD^-1 mod PAIR_P, whose
-// residues mod 61 and mod 67 are the two primes' own starts.  Primes 2..82
-// follow, one bitstring each.
+// rounded up to an even word count.  The first four primes are held in two
+// pair bitstrings, of periods 61 * 67 (PAIR1_P) and 71 * 73 (PAIR2_P): bit j
+// of a pair's string is B_p[j] & B_q[j], and a lattice value's window in it
+// starts at n59 * MOD^-1 mod (p*q), whose residues mod p and mod q are the
+// two primes' own starts.  Primes 4..82 follow, one bitstring each.
 constexpr int WIN_EXTRA = 672;
-constexpr int PAIR_P = 61 * 67;                      // 4087
+constexpr int PAIR1_P = 61 * 67;                     // 4087
+constexpr int PAIR2_P = 71 * 73;                     // 5183
 constexpr int nwords(int p) { return ((p + WIN_EXTRA + 31) / 32 + 1) & ~1; }
-constexpr int PAIR_WORDS = nwords(PAIR_P);           // 150
-constexpr int word_offset(int g) {                   // g >= 2
-  int o = PAIR_WORDS;
-  for (int i = 2; i < g; i++) o += nwords(PRIMES[i]);
+constexpr int PAIR1_WORDS = nwords(PAIR1_P);         // 150
+constexpr int PAIR2_WORDS = nwords(PAIR2_P);         // 184
+constexpr int PAIR_PRIMES = 4;                       // primes held in the pairs
+constexpr int word_offset(int g) {                   // g >= PAIR_PRIMES
+  int o = PAIR1_WORDS + PAIR2_WORDS;
+  for (int i = PAIR_PRIMES; i < g; i++) o += nwords(PRIMES[i]);
   return o;
 }
-constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2670 words, 10680 bytes
+constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2806 words, 11224 bytes
 
 // Lattice order.  The 12673 n53 starts of one n43 value (index j43*667 +
-// j47*29 + j53) are visited sorted by their window start in the pair
-// bitstring, (j43*d43 + j47*d47 + j53*d53) mod PAIR_P with d = S * MOD^-1
-// mod PAIR_P; the 32 starts of a warp then lie within a few bits of each
-// other there (12673 starts over 4087 residues, plus at most 3 for the
-// reductions mod MOD), so the pair bitstring's words are read without bank
-// conflicts.  The order is one 16-bit index per start, built with the tables.
+// j47*29 + j53) are visited sorted by their window starts in the pair
+// bitstrings: the start in the 61*67 string is k1 = (j43*d43 + j47*d47 +
+// j53*d53) mod 4087 (d = S * MOD^-1 mod 4087) up to the reductions mod MOD
+// (at most 3), and k2 likewise mod 5183.  Starts are ordered by k1 in
+// buckets of ORDER_BUCKET values, and by k2 inside a bucket (about 320
+// starts each).  The 32 starts of a warp then lie within about 230 bits of
+// each other in the first string and 870 bits in the second, a half warp
+// within half that, so neither pair bitstring's 64-bit loads conflict.  The
+// order is one 16-bit index per start, built with the tables.
+constexpr int ORDER_BUCKET = 103;
 constexpr int PERM_WORDS = (N53_PER_N43 + 1) / 2;   // 6337 words
-constexpr int JOB_TABLE_WORDS = TABLE_WORDS + PERM_WORDS;   // per K-job, 36,068 bytes
+constexpr int JOB_TABLE_WORDS = TABLE_WORDS + PERM_WORDS;   // per K-job, 36,572 bytes
 
 constexpr int64_t mod_pos(int64_t a, int64_t m) { return ((a % m) + m) % m; }
 constexpr int inv_mod(int a, int p) {                // a^-1 mod p, a coprime to p
@@ -87,8 +94,8 @@ constexpr int ilog2(int x) { int k = 0; while ((2 << k) <= x) k++; return k; }
 //   M = ceil(2^(32+k) / p) < 2^32,
 // is exact for every x < 2^31 (round-up reciprocal, error x*(M*p-2^(32+k))
 // / (p*2^(32+k)) < 1/p).
-// For the pair bitstring (p = 4087) x < 3 * 2^16 * 4087 < 2^30 and the
-// error bound x / 2^43 < 1/4087 holds the same way.
+// For the pair bitstrings (p = 4087, 5183) x < 3 * 2^16 * 5183 < 2^30, and
+// the reduction was checked exhaustively for every x < 2^30 with both.
 struct PrimeParam {
   int p, A, B, C, k, off;
   uint32_t M;
@@ -102,14 +109,17 @@ constexpr PrimeParam make_param_p(int p, int off) {
   uint64_t M = ((uint64_t)1 << (32 + k)) / (uint64_t)p + 1;
   return PrimeParam{p, A, B, C, k, off, (uint32_t)M};
 }
-// Prime g's own bitstring (g >= 2; primes 0 and 1 only exist in the pair).
+// Prime g's own bitstring (g >= 4; primes 0..3 only exist in the pairs).
 constexpr PrimeParam make_param(int g) {
-  return make_param_p(PRIMES[g], g >= 2 ? word_offset(g) : 0);
+  return make_param_p(PRIMES[g], g >= PAIR_PRIMES ? word_offset(g) : 0);
 }
-constexpr PrimeParam PAIR_PARAM = make_param_p(PAIR_P, 0);
-// Dense-phase windows: unit 0 is the pair bitstring (primes 0 and 1), unit
-// u >= 1 is prime u + 1.
-constexpr PrimeParam dense_param(int u) { return u == 0 ? PAIR_PARAM : make_param(u + 1); }
+constexpr PrimeParam PAIR1_PARAM = make_param_p(PAIR1_P, 0);
+constexpr PrimeParam PAIR2_PARAM = make_param_p(PAIR2_P, PAIR1_WORDS);
+// Dense-phase windows: units 0 and 1 are the pair bitstrings (primes 0..3),
+// unit u >= 2 is prime u + 2.
+constexpr PrimeParam dense_param(int u) {
+  return u == 0 ? PAIR1_PARAM : u == 1 ? PAIR2_PARAM : make_param(u + 2);
+}
 
 // Residue 0 test helpers for the 7..23 filter (sieve.cl:123-142,
 // cpusse2.cpp:563-568).

@@ -32,14 +32,14 @@
 // conflict-free: all lanes read the same prime's string at word offsets
 // that differ by at most (p-1)/32 < 17, i.e. inside one 32-bank row.
 // Primes 61 and 67 share one string of period 4087 (bit j = B_61[j] &
-// B_67[j], window start n59 * MOD^-1 mod 4087); its windows are read
-// conflict-free because the starts of an n43 value are visited sorted by
-// that window start (ap26_const.cuh), so a warp's 32 starts lie within a
-// few words of each other.
+// B_67[j], window start n59 * MOD^-1 mod 4087), and 71 and 73 one of
+// period 5183; their windows are read conflict-free because the starts of
+// an n43 value are visited sorted by those window starts (ap26_const.cuh),
+// so a warp's 32 starts lie close together in both strings.
 //
-//   dense phase  the first G primes for all 10 words of every n59: G-1
-//                windows (the pair, primes 2..G-1), each 21 word loads +
-//                20 funnel shifts
+//   dense phase  the first G primes for all 10 words of every n59: G-2
+//                windows (the two pairs, primes 4..G-1), each 21 word loads
+//                + 20 funnel shifts
 //   tail         live (n59, word) pairs are compacted into a per-warp shared
 //                queue (ballot/popc) and advanced R primes at a time, all
 //                lanes on the same prime, until stage SL
@@ -159,26 +159,6 @@ __device__ __forceinline__ uint32_t unit_start(uint32_t a, uint32_t b, uint32_t 
   return x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k);
 }
 
-// All 640 bits (20 words) of dense unit u ANDed into acc: 11 pair loads, 20
-// funnel shifts.
-template <int u>
-__device__ __forceinline__ void dense_unit(const uint32_t *__restrict__ tab, uint32_t a,
-                                           uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
-  constexpr PrimeParam P = dense_param(u);
-  const uint32_t s = unit_start<u>(a, b, c);
-  const uint2 *t = pair_at(tab, P.off, s >> 5);
-  const uint32_t sh = s & 31;
-  uint32_t v[22];
-#pragma unroll
-  for (int i = 0; i < 11; i++) {
-    const uint2 w = t[2 * i];
-    v[2 * i] = w.x;
-    v[2 * i + 1] = w.y;
-  }
-#pragma unroll
-  for (int i = 0; i < 20; i++) acc[i] &= __funnelshift_r(v[i], v[i + 1], sh);
-}
-
 // Units u and u+1 together: acc &= window_u & window_{u+1}, one 3-input
 // LOP3 per word instead of two ANDs.
 template <int u>
@@ -210,15 +190,13 @@ __device__ __forceinline__ void dense_twos(const uint32_t *tab, uint32_t a, uint
   (dense_two<2 * I>(tab, a, b, c, acc), ...);
 }
 
-// The first G primes (G even): the pair bitstring (primes 0 and 1) and
-// primes 2..G-1, G-1 windows, in twos and one last single.
+// The first G primes (G even): the two pair bitstrings (primes 0..3) and
+// primes 4..G-1, G-2 windows, two at a time.
 template <int G>
 __device__ __forceinline__ void dense_all(const uint32_t *tab, uint32_t a, uint32_t b,
                                           uint32_t c, uint32_t (&acc)[20]) {
-  static_assert(G % 2 == 0 && G >= 4, "dense phase: the pair and an odd number of primes");
-  constexpr int U = G - 1;
-  dense_twos(tab, a, b, c, acc, std::make_integer_sequence<int, U / 2>{});
-  dense_unit<U - 1>(tab, a, b, c, acc);
+  static_assert(G % 2 == 0 && G >= 6, "dense phase: both pairs and an even number of primes");
+  dense_twos(tab, a, b, c, acc, std::make_integer_sequence<int, (G - 2) / 2>{});
 }
 
 // Queue item: x = n59 bits 0..31, y = n59 bits 32..47 | w << 16, z/w = mask.

@@ -238,7 +238,7 @@ int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
  * ap26_serve_submit admits a unit (its id unique among the units admitted and
  * not yet polled, AP26_E_ARG otherwise) while device memory allows, else
  * returns AP26_E_NOMEM: the unit holds one table per K on the device (the
- * K's sieve bitstrings and lattice order, 36,028 bytes) from admission to
+ * K's sieve bitstrings and lattice order, 36,572 bytes) from admission to
  * completion, in a pool sized from
  * ap26_opts.mem_budget at the first admission, together with its checkpoint
  * slot (at most 1024 units at once).  Admission enqueues the unit's tables
@@ -319,7 +319,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  * valid once that stream reaches this point.
  * - Allocates nothing (no cudaMalloc/cudaFree, no context object): all
  *   scratch -- job descriptors, tables, counters -- lives in one
- *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (2,314,608 bytes)
+ *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (2,349,424 bytes)
  *   that every GPU loading the library keeps until process exit.  At most
  *   AP26_NOALLOC_MAX_K values of K per call; more returns AP26_E_CAPACITY.
  *   An invalid K costs no sieve time.
@@ -333,7 +333,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  *   calls whose work overlaps on the GPU (other streams, other threads)
  *   race on it and must be serialised by the caller. */
 #define AP26_NOALLOC_MAX_K 64
-#define AP26_NOALLOC_SCRATCH_BYTES 2314608
+#define AP26_NOALLOC_SCRATCH_BYTES 2349424
 int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
                              int64_t *d_counts, void *stream);
 

@@ -187,13 +187,13 @@ def test_admission_by_device_memory():
 
 
 def test_densest_k_runs_and_serves_without_overflow():
-    """K = 61*67*71*73 = 21182107 is the densest searchable K below 4e8: the
+    """K = 61*67*71*73 = 21182921 is the densest searchable K below 4e8: the
     four smallest sieve primes divide K*23#, so each bans one residue
     instead of 24 and about 5.4 times the usual candidates survive.  The
     synchronous search redoes an overflowing chunk in smaller ones (here a
     2^24-entry ring forces it); serving slices size their chunks for this
     density.  Both give the reference's reports."""
-    K = 21182107
+    K = 21182921
     ref = ref_raw(K)
     with A.Context(0, cand_ring_log2=24) as c:
         aps, st = c.search_k(K, 0)
