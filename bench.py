@@ -53,6 +53,14 @@ def will_search(k):
     return all(k % p for p in (29, 31, 37, 41, 43, 47, 53, 59))
 
 
+_T0 = time.time()
+
+
+def progress(msg):
+    """One line per phase on stderr, so a slow phase shows where it is."""
+    print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 # ---- clocks during the timed region -------------------------------------------
 class ClockSampler:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -441,7 +449,11 @@ def measure_serve(ctx, A, capacity_kps, roofline_kps, n_units=SERVE_UNITS, max_k
     lat, res_of = {}, {}
     t0 = time.perf_counter()
     nxt, done, total_k = 0, 0, 0
+    limit_s = 60.0 + 4.0 * sum(ks_of.values()) / max(capacity_kps, 0.1)
     while done < len(units):
+        if time.perf_counter() - t0 > limit_s:
+            raise RuntimeError(f"serving did not finish in {limit_s:.0f} s: {done} of "
+                               f"{len(units)} units returned, {nxt} submitted")
         now = time.perf_counter() - t0
         while nxt < len(units) and arrivals[nxt] <= now:
             rc = ctx.serve_submit(*units[nxt])
@@ -602,11 +614,13 @@ def main():
     import ap26_b200 as A
     from ap26_b200 import replicas
 
-    ctx = A.Context(local, profile=1)
+    ctx = A.Context(local, profile=1, wait_timeout_s=300.0)
+    progress("context created")
     tuned = None
     if not args.no_autotune:
         tuned = ctx.autotune(KMIN_SEEDED + 64 * rank if will_search(KMIN_SEEDED + 64 * rank)
                              else KMIN_SEEDED)
+    progress(f"autotuned: {tuned}")
     smem_gbs, int_tops = ctx.probe_peaks()
     roofline_kps = smem_gbs * 1e9 / ALG_BYTES_PER_K
     kmin, _ = replicas.rank_range(KMIN_SEEDED, RANGE_K, rank)
@@ -649,6 +663,7 @@ def main():
     for i in range(args.warmup):
         run_step(i, [])
     seen.clear()
+    progress("warm-up steps done")
 
     def barrier():
         torch.cuda.synchronize()
@@ -680,6 +695,7 @@ def main():
         wall = time.perf_counter() - t0
     ev_ms = ev0.elapsed_time(ev1)
     raw_k = STEP_K * args.steps
+    progress(f"timed steps done: {tot['ks']} K in {wall:.1f} s")
 
     vec = torch.tensor([tot["dev_ms"], wall, ev_ms, tot["sieve_ms"]], dtype=torch.float64,
                        device="cuda")
@@ -706,6 +722,7 @@ def main():
         if world > 1:
             dist.all_reduce(pv, op=dist.ReduceOp.MAX)
             dist.all_reduce(pkt, op=dist.ReduceOp.SUM)
+        progress("plain form done")
         plain = {"value": pkt.item() / (pv[0].item() / 1000.0), "unit": "K/s",
                  "e2e": pkt.item() / pv[1].item(), "searched_k": int(pkt.item()),
                  "form": "ap26_search_k_sol per K over the 64-K range (search + ReportSolution "
@@ -719,6 +736,7 @@ def main():
                 secondary[name] = fn()
             except Exception as e:          # noqa: BLE001
                 secondary[name] = {"error": f"{type(e).__name__}: {e}"}
+            progress(f"{name} done")
 
         with ClockSampler(local) as clk2:
             keep("batched", lambda: measure_batched(ctx, A, n_items=args.batched_items))
@@ -790,6 +808,7 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             ks = [k for k in range(KMIN_SEEDED, KMIN_SEEDED + RANGE_K) if will_search(k)]
             cb = cpu_baseline_value(ks, 6)
+            progress("cpu baseline done")
             cb["extrapolated"] = ("per-pass time per lattice value from a bounded sample, "
                                   "times the 10840 lattice values of a pass, plus set-up; "
                                   "checked once against a whole K (591 s estimated, 614 s "
