@@ -1063,6 +1063,10 @@ static int collect_run(ap26_ctx *ctx, JobSet &S, cudaStream_t cs, ap26_stats *st
   }
   if (n_aps_out) *n_aps_out = n_aps;
   const unsigned err = S.h_st->err_flags;
+  if (err & ERR_CHAIN_LIMIT) {
+    ctx->last_error = "a chain walk reached its test limit (corrupt candidate data)";
+    return AP26_E_CUDA;
+  }
   if (err & ERR_DOMAIN) {
     ctx->last_error = "chain term reached 2^62";
     return AP26_E_DOMAIN;

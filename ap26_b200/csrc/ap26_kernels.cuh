@@ -95,6 +95,7 @@ enum : unsigned int {
   ERR_CAND_OVERFLOW = 1u,
   ERR_DOMAIN = 4u,
   ERR_AP_OVERFLOW = 8u,
+  ERR_CHAIN_LIMIT = 16u,   // a chain walk ran kMaxChainTests tests: bad candidate data
 };
 
 struct SieveArgs {
@@ -586,13 +587,18 @@ __device__ __forceinline__ void emit_chain(const ChainArgs &A, int k, int job, i
   }
 }
 
+// No AP of valid candidates comes near this length (the longest known has 27
+// terms); a walk that reaches it ends with ERR_CHAIN_LIMIT, so the kernel
+// ends whatever its input holds.
+constexpr int kMaxChainTests = 4096;
+
 __global__ void chain_kernel(ChainArgs A) {
   const unsigned long long n_c = min(*A.cand_count, (unsigned long long)A.cand_cap);
   const int lane = threadIdx.x & 31;
   unsigned tests = 0, sq = 0;
   bool active = false, bwd = false;
   int64_t n = 0, m = 0, S = 0;
-  int k = 0, job = 0;
+  int k = 0, job = 0, walk = 0;
   unsigned long long base = 0;
   int left = 0;                 // unclaimed-by-lane candidates of the warp's batch
   bool exhausted = false;
@@ -621,12 +627,17 @@ __global__ void chain_kernel(ChainArgs A) {
         S = A.jobs[job].STEP;
         m = n + S * 5;
         k = 0;
+        walk = 0;
         bwd = false;
         active = true;
       }
       left -= take;
     }
     if (!__any_sync(FULL, active)) break;
+    if (active && ++walk > kMaxChainTests) {
+      atomicOr(&A.st->err_flags, ERR_CHAIN_LIMIT);
+      active = false;
+    }
     if (active) {
       if (bwd && m <= 0) {          // the backward walk stops below zero, untested
         emit_chain(A, k, job, m + S, n);

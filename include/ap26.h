@@ -103,7 +103,8 @@ typedef struct {
   double device_ms;     /* CUDA-event time of the device work                */
   int32_t error_flags;  /* bit 0: candidate buffer overflow (retried), bit 1:
                            late buffer overflow (retried), bit 2: chain term
-                           >= 2^62, bit 3: AP buffer overflow                */
+                           >= 2^62, bit 3: AP buffer overflow, bit 4: a chain
+                           walk reached its 4096-test limit (corrupt data) */
   int32_t launches;     /* kernels launched for this call                    */
   double sieve_ms;      /* summed CUDA-event time of the sieve launches
                            (only with ap26_opts.profile = 1)                 */
