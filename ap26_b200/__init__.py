@@ -53,7 +53,7 @@ class Stats(ctypes.Structure):
                 ("device_ms", ctypes.c_double), ("error_flags", ctypes.c_int32),
                 ("launches", ctypes.c_int32), ("sieve_ms", ctypes.c_double),
                 ("sieve_cells", ctypes.c_int64), ("sieve_launches", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("reserved", ctypes.c_int32), ("chain_walks", ctypes.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

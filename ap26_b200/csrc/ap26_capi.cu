@@ -1030,6 +1030,7 @@ static int collect_run(ap26_ctx *ctx, JobSet &S, cudaStream_t cs, ap26_stats *st
     stats->candidates = (int64_t)S.h_st->cand_total;
     stats->late_items = (int64_t)S.h_st->late_items;
     stats->prp_tests = (int64_t)S.h_st->prp_tests;
+    stats->chain_walks = (int64_t)S.h_st->chain_walks;
     stats->aps = (int64_t)S.h_st->ap_count;
     stats->device_ms = ms;
     stats->error_flags = (int32_t)S.h_st->err_flags;
@@ -1065,6 +1066,10 @@ static int collect_run(ap26_ctx *ctx, JobSet &S, cudaStream_t cs, ap26_stats *st
   const unsigned err = S.h_st->err_flags;
   if (err & ERR_CHAIN_LIMIT) {
     ctx->last_error = "a chain walk reached its test limit (corrupt candidate data)";
+    return AP26_E_CUDA;
+  }
+  if (!S.count_only && S.h_st->chain_check != 0) {
+    ctx->last_error = "the chain walk did not take each candidate exactly once";
     return AP26_E_CUDA;
   }
   if (err & ERR_DOMAIN) {

@@ -89,6 +89,9 @@ struct DevState {
   unsigned long long ap_count, prp_tests, cand_total, late_items;  // per run
   unsigned int err_flags;
   unsigned int pad;
+  unsigned long long chain_walks;              // candidates the chain walk took, per run
+  unsigned long long chain_check;              // sum of n over the rings' filled entries
+                                               // minus sum of n over the walked ones: 0
 };
 
 enum : unsigned int {
@@ -595,12 +598,19 @@ constexpr int kMaxChainTests = 4096;
 __global__ void chain_kernel(ChainArgs A) {
   const unsigned long long n_c = min(*A.cand_count, (unsigned long long)A.cand_cap);
   const int lane = threadIdx.x & 31;
-  unsigned tests = 0, sq = 0;
+  unsigned tests = 0, sq = 0, walks = 0;
+  // coverage check: each of the ring's n_c filled entries is walked once, so
+  // the sum of their n minus the sum of the walked n is 0 (mod 2^64)
+  unsigned long long chk = 0;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_c;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    chk += (unsigned long long)A.cand[i].n;
   bool active = false, bwd = false;
   int64_t n = 0, m = 0, S = 0;
   int k = 0, job = 0, walk = 0;
   unsigned long long base = 0;
-  int left = 0;                 // unclaimed-by-lane candidates of the warp's batch
+  int got = 0;                  // candidates in the warp's current batch (<= 32)
+  int left = 0;                 // of them, not yet taken by a lane
   bool exhausted = false;
   for (;;) {
     // refill: idle lanes take the next candidates of the warp's batch
@@ -613,6 +623,7 @@ __global__ void chain_kernel(ChainArgs A) {
         b = __shfl_sync(FULL, b, 0);
         base = b;
         left = b < n_c ? (int)min(32ull, n_c - b) : 0;
+        got = left;
         if (left == 0) {
           exhausted = true;
           break;
@@ -621,13 +632,15 @@ __global__ void chain_kernel(ChainArgs A) {
       const int rank = __popc(idle & ((1u << lane) - 1u));
       const int take = min(__popc(idle), left);
       if (!active && rank < take) {
-        const Cand cd = A.cand[base + (32 - left) + rank];
+        const Cand cd = A.cand[base + (got - left) + rank];
         n = cd.n;
         job = cd.job;
+        chk -= (unsigned long long)n;
         S = A.jobs[job].STEP;
         m = n + S * 5;
         k = 0;
         walk = 0;
+        walks++;
         bwd = false;
         active = true;
       }
@@ -654,10 +667,16 @@ __global__ void chain_kernel(ChainArgs A) {
       }
     }
   }
-  // warp-aggregated test counter
-  unsigned v = tests;
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  // warp-aggregated test and walk counters
+  unsigned v = tests, w = walks;
+  for (int o = 16; o; o >>= 1) {
+    v += __shfl_xor_sync(FULL, v, o);
+    w += __shfl_xor_sync(FULL, w, o);
+    chk += __shfl_xor_sync(FULL, chk, o);
+  }
   if (lane == 0 && v) atomicAdd(&A.st->prp_tests, (unsigned long long)v);
+  if (lane == 0 && w) atomicAdd(&A.st->chain_walks, (unsigned long long)w);
+  if (lane == 0 && chk) atomicAdd(&A.st->chain_check, chk);
 }
 
 // ---- ReportSolution on the device: AP26.cpp:484-602 ------------------------------

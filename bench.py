@@ -45,7 +45,7 @@ N59_PER_K = 4808136200          # lattice positions per K (10840 n43 x 443555)
 CONSULTS_PER_WORD = 16.62       # oracle: mean table lookups per shift word (canonical order)
 BYTES_PER_CONSULT = 8
 # H2D/D2H payload per K-job and per call (sizes of the C ABI structures)
-KJOB_BYTES, DEVSTATE_BYTES, APREC_BYTES, COUNT_BYTES, FINAL_BYTES = 128, 112, 24, 8, 56
+KJOB_BYTES, DEVSTATE_BYTES, APREC_BYTES, COUNT_BYTES, FINAL_BYTES = 128, 128, 24, 8, 56
 REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 
 
@@ -450,7 +450,11 @@ def measure_serve(ctx, A, capacity_kps, roofline_kps, n_units=SERVE_UNITS, max_k
     t0 = time.perf_counter()
     nxt, done, total_k = 0, 0, 0
     limit_s = 60.0 + 4.0 * sum(ks_of.values()) / max(capacity_kps, 0.1)
+    last = 0.0
     while done < len(units):
+        if time.perf_counter() - t0 - last > 10.0:
+            last = time.perf_counter() - t0
+            progress(f"serving: {nxt} of {len(units)} units submitted, {done} returned")
         if time.perf_counter() - t0 > limit_s:
             raise RuntimeError(f"serving did not finish in {limit_s:.0f} s: {done} of "
                                f"{len(units)} units returned, {nxt} submitted")
@@ -479,7 +483,7 @@ def measure_serve(ctx, A, capacity_kps, roofline_kps, n_units=SERVE_UNITS, max_k
     span = time.perf_counter() - t0
     ls = sorted(lat.values())
     # latency at the roofline: the unit's K alone at the sieve's shared-memory roofline
-    frac = sorted(ks_of[i] / roofline_kps / lat[i] for i in lat)
+    frac = sorted(ks_of[i] / roofline_kps / lat[i] for i in lat if ks_of[i])
     par = item_parity(A, units, [res_of[u[0]][1] for u in units],
                       [res_of[u[0]][0].result_hash for u in units])
     return {
@@ -493,8 +497,9 @@ def measure_serve(ctx, A, capacity_kps, roofline_kps, n_units=SERVE_UNITS, max_k
         "sustained_frac_of_roofline": total_k / span / roofline_kps,
         "latency_frac_of_roofline": {"p50": float(np.percentile(frac, 50)),
                                      "p1": float(np.percentile(frac, 1)),
-                                     "note": "per unit: its K at the sieve roofline alone "
-                                             "/ measured completion latency"},
+                                     "note": "per unit with a searchable K: its K at the "
+                                             "sieve roofline alone / measured completion "
+                                             "latency"},
         "parity": par,
     }
 

@@ -111,6 +111,8 @@ typedef struct {
   int64_t sieve_cells;  /* (lattice value, shift word) cells sieved          */
   int32_t sieve_launches;
   int32_t reserved;
+  int64_t chain_walks;  /* candidates the chain walk took (equals candidates
+                           when no candidate buffer overflowed)             */
 } ap26_stats;
 
 /* A work item: every searchable K in [kmin, kmax] at one SHIFT. */
@@ -320,7 +322,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  * valid once that stream reaches this point.
  * - Allocates nothing (no cudaMalloc/cudaFree, no context object): all
  *   scratch -- job descriptors, tables, counters -- lives in one
- *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (2,349,424 bytes)
+ *   file-scope device array of AP26_NOALLOC_SCRATCH_BYTES (2,349,440 bytes)
  *   that every GPU loading the library keeps until process exit.  At most
  *   AP26_NOALLOC_MAX_K values of K per call; more returns AP26_E_CAPACITY.
  *   An invalid K costs no sieve time.
@@ -334,7 +336,7 @@ int ap26_chain_batch(ap26_ctx *ctx, int K, const int64_t *n, int64_t count,
  *   calls whose work overlaps on the GPU (other streams, other threads)
  *   race on it and must be serialised by the caller. */
 #define AP26_NOALLOC_MAX_K 64
-#define AP26_NOALLOC_SCRATCH_BYTES 2349424
+#define AP26_NOALLOC_SCRATCH_BYTES 2349440
 int ap26_sieve_count_noalloc(int device, const int32_t *d_Ks, int nK, int shift,
                              int64_t *d_counts, void *stream);
 

@@ -209,6 +209,28 @@ def test_recorded_reference_ranges(ctx):
             assert st.candidates == pinned[(K, shift)], (K, shift)
 
 
+def test_chain_walk_takes_each_candidate_once_after_other_runs():
+    """The chain walk takes every filled entry of its candidate ring once and
+    nothing past the fill count: a ring keeps the previous runs' entries
+    (here a batch of 9 K, then a smaller K), and a walk of a stale entry
+    would use another run's job index.  The device checks coverage itself
+    (sum of n over the filled entries minus sum over the walked ones; the
+    call fails if it is not 0); the walk count equals the survivor count."""
+    with A.Context(0) as c:
+        per, res, st0 = c.search_batch([(1, 1000037, 1000048, 640)])
+        assert st0.chain_walks == st0.candidates > 0
+        for K, shift in ((366384, 0), (43241061, 0)):
+            aps, st = c.search_k(K, shift)
+            assert st.chain_walks == st.candidates > 0
+            assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(K, shift)
+        # one-K chunks whose last batch of 32 is partial, in a ring that
+        # still holds longer runs' entries
+        c.set_opts(chunk_tiles=4099)
+        aps, st = c.search_k(366384, 0)
+        assert st.chain_walks == st.candidates == 38838420
+        assert [(k, KK, f) for k, KK, f, _ in aps] == ref_raw(366384)
+
+
 def test_search_k_rejects_unsearchable_and_out_of_domain(ctx):
     with pytest.raises(A.AP26Error):
         ctx.search_k(29 * 1000)
