@@ -289,7 +289,7 @@ struct SieveVariant {
   int G, R, SL, QCAP, LCAP, WARPS;
   void (*kernel)(SieveArgs);
   size_t smem() const {
-    return sizeof(uint4) * (QCAP + LCAP) * WARPS + 2 * sizeof(uint32_t) * TABLE_WORDS;
+    return sizeof(uint4) * (QCAP + LCAP) * WARPS + (size_t)table_bytes(G);
   }
 };
 

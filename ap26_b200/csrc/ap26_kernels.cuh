@@ -147,13 +147,21 @@ __device__ __forceinline__ int64_t mod_MOD(uint64_t x) {
 }
 
 // ---- sieve pieces -----------------------------------------------------------
-// The shared table holds the bitstrings as overlapping 64-bit pairs:
-// pair[i] = (word i, word i+1) for every i, so a window starting at any word
-// is a run of aligned 64-bit loads, pair[w], pair[w+2], ...; for a warp the
-// pairs read at one step lie within (p-1)/32 + 1 consecutive entries
-// (distinct banks or broadcast).
-__device__ __forceinline__ const uint2 *pair_at(const uint32_t *tab, uint32_t off, uint32_t w) {
-  return reinterpret_cast<const uint2 *>(tab) + off + w;
+// The shared table holds the bitstrings in two regions.  The dense primes'
+// words [0, D), D = word_offset(G), come first as overlapping 128-bit quads,
+// quad[i] = (word i .. word i+3), so a 640-bit window starting at any word
+// is five aligned 128-bit loads and one 32-bit load; a quarter warp's quads
+// at one step lie within (p-1)/32 + 1 < 8 consecutive entries (distinct
+// banks or broadcast).  The tail primes' words [D, TABLE_WORDS) follow once
+// each: a 64-bit window at any bit is three 32-bit loads, and a warp's loads
+// for one prime lie within floor((p + 575)/32) + 3 consecutive words, at
+// most 32 (conflict-free) for every p below 385.
+constexpr int table_bytes(int G) {
+  return 16 * word_offset(G) + 4 * (TABLE_WORDS - word_offset(G));
+}
+
+__device__ __forceinline__ const uint4 *quad_at(const uint32_t *tab, uint32_t off, uint32_t w) {
+  return reinterpret_cast<const uint4 *>(tab) + off + w;
 }
 
 template <int u>
@@ -170,18 +178,24 @@ __device__ __forceinline__ void dense_two(const uint32_t *__restrict__ tab, uint
                                           uint32_t b, uint32_t c, uint32_t (&acc)[20]) {
   constexpr PrimeParam P = dense_param(u), Q = dense_param(u + 1);
   const uint32_t s = unit_start<u>(a, b, c), t = unit_start<u + 1>(a, b, c);
-  const uint2 *tp = pair_at(tab, P.off, s >> 5);
-  const uint2 *tq = pair_at(tab, Q.off, t >> 5);
+  const uint4 *tp = quad_at(tab, P.off, s >> 5);
+  const uint4 *tq = quad_at(tab, Q.off, t >> 5);
   const uint32_t sp = s & 31, sq = t & 31;
-  uint32_t vp[22], vq[22];
+  uint32_t vp[21], vq[21];
 #pragma unroll
-  for (int i = 0; i < 11; i++) {
-    const uint2 x = tp[2 * i], y = tq[2 * i];
-    vp[2 * i] = x.x;
-    vp[2 * i + 1] = x.y;
-    vq[2 * i] = y.x;
-    vq[2 * i + 1] = y.y;
+  for (int i = 0; i < 5; i++) {
+    const uint4 x = tp[4 * i], y = tq[4 * i];
+    vp[4 * i] = x.x;
+    vp[4 * i + 1] = x.y;
+    vp[4 * i + 2] = x.z;
+    vp[4 * i + 3] = x.w;
+    vq[4 * i] = y.x;
+    vq[4 * i + 1] = y.y;
+    vq[4 * i + 2] = y.z;
+    vq[4 * i + 3] = y.w;
   }
+  vp[20] = *reinterpret_cast<const uint32_t *>(tp + 20);
+  vq[20] = *reinterpret_cast<const uint32_t *>(tq + 20);
 #pragma unroll
   for (int i = 0; i < 20; i++)
     acc[i] &= __funnelshift_r(vp[i], vp[i + 1], sp) & __funnelshift_r(vq[i], vq[i + 1], sq);
@@ -238,19 +252,19 @@ __device__ __forceinline__ int emit_word(const SieveArgs &A, uint64_t n59, int w
 
 // One word of prime P (runtime parameters, identical for all lanes): the 64
 // bits of the window at pos..pos+63, i.e. words j, j+1, j+2 (j = pos / 32)
-// funnel-shifted by pos mod 32, read as pair j and the low half of pair j+2.
+// funnel-shifted by pos mod 32.  `tab` is the tail region's base moved back
+// by D words, so a tail prime's global word offset indexes it directly.
 __device__ __forceinline__ void word_prime_rt(const uint32_t *__restrict__ tab,
                                               const PrimeParam &P, uint32_t a, uint32_t b,
                                               uint32_t c, uint32_t w64, uint32_t &lo,
                                               uint32_t &hi) {
   const uint32_t x = a * (uint32_t)P.A + b * (uint32_t)P.B + c * (uint32_t)P.C;
   const uint32_t pos = x - (uint32_t)P.p * (__umulhi(x, P.M) >> P.k) + w64;
-  const uint32_t w = pos >> 5;
+  const uint32_t *v = tab + (uint32_t)P.off + (pos >> 5);
   const uint32_t sh = pos & 31;
-  const uint2 u = *pair_at(tab, (uint32_t)P.off, w);
-  const uint32_t v2 = pair_at(tab, (uint32_t)P.off, w + 2)->x;
-  lo &= __funnelshift_r(u.x, u.y, sh);
-  hi &= __funnelshift_r(u.y, v2, sh);
+  const uint32_t v0 = v[0], v1 = v[1], v2 = v[2];
+  lo &= __funnelshift_r(v0, v1, sh);
+  hi &= __funnelshift_r(v1, v2, sh);
 }
 
 // Tail stages g_begin..g_end-1: every queued item advances R primes per pass
@@ -395,6 +409,9 @@ sieve_kernel(SieveArgs A) {
   uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
   uint4 *lqueues = queues + QCAP * WARPS;
   uint32_t *tab = reinterpret_cast<uint32_t *>(lqueues + LCAP * WARPS);
+  constexpr int D = word_offset(G);
+  static_assert(D + 3 <= TABLE_WORDS, "quad entries read past the table");
+  uint32_t *ptab = tab + 3 * D;   // tail words: ptab[off + w], off >= D
   __shared__ unsigned long long s_tile;
   __shared__ int s_job;
   __shared__ unsigned long long s_kept[WARPS];
@@ -426,7 +443,7 @@ sieve_kernel(SieveArgs A) {
     if (job != cur_job || job < 0) {
       if (cur_job >= 0) {
         // finish the previous job's items with its table still in place
-        kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift,
+        kept_acc += front_drain<G, R, SL, LCAP>(A, ptab, q, cnt, lq, lcnt, lane, cur_shift,
                                                 cur_job, late_acc, true);
         const unsigned long long v = warp_sum(kept_acc);
         if (lane == 0) s_kept[warp] = v;
@@ -442,10 +459,9 @@ sieve_kernel(SieveArgs A) {
       const uint32_t *src = A.tables + (size_t)A.jobs[job].table * JOB_TABLE_WORDS;
       cur_perm = (A.jobs[job].flags & JOB_SORTED)
                      ? reinterpret_cast<const uint16_t *>(src + TABLE_WORDS) : nullptr;
-      for (int i = threadIdx.x; i < TABLE_WORDS; i += blockDim.x) {
-        tab[2 * i] = src[i];
-        tab[2 * i + 1] = (i + 1 < TABLE_WORDS) ? src[i + 1] : 0u;
-      }
+      for (int i = threadIdx.x; i < D; i += blockDim.x)   // D + 3 <= TABLE_WORDS
+        reinterpret_cast<uint4 *>(tab)[i] = make_uint4(src[i], src[i + 1], src[i + 2], src[i + 3]);
+      for (int i = D + threadIdx.x; i < TABLE_WORDS; i += blockDim.x) ptab[i] = src[i];
       cur_job = job;
       cur_shift = A.jobs[job].shift;
       __syncthreads();
@@ -474,7 +490,7 @@ sieve_kernel(SieveArgs A) {
         incoming += __popc(bal[w]);
       }
       if (cnt + incoming > QCAP)
-        kept_acc += front_drain<G, R, SL, LCAP>(A, tab, q, cnt, lq, lcnt, lane, cur_shift, job,
+        kept_acc += front_drain<G, R, SL, LCAP>(A, ptab, q, cnt, lq, lcnt, lane, cur_shift, job,
                                                 late_acc, false);
 #pragma unroll
       for (int w = 0; w < WORDS; w++) {
