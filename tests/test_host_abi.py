@@ -1,6 +1,7 @@
 """CPU tests of libap26.so: it loads, exports every symbol include/ap26.h
 declares, refuses to run without a GPU (no CPU fallback), and its host
 services reproduce the reference's SOL files, hash and state files."""
+import ctypes
 import os
 import re
 import subprocess
@@ -120,3 +121,30 @@ def test_cli_without_gpu_exits_nonzero(tmp_path):
                        text=True)
     assert p.returncode != 0
     assert not (tmp_path / "SOL-AP26.txt").exists()
+
+
+@pytest.mark.parametrize("cname,pyname", [
+    ("ap26_opts", "Opts"), ("ap26_ap", "AP"), ("ap26_stats", "Stats"), ("ap26_item", "Item"),
+    ("ap26_item_result", "ItemResult"), ("ap26_final", "Final"), ("ap26_sol", "Sol")])
+def test_ctypes_structures_match_the_header(tmp_path, cname, pyname):
+    """Every ctypes mirror has the C struct's size and field offsets, as
+    include/ap26.h declares them (compiled here with the host C compiler)."""
+    import shutil
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    py = getattr(A, pyname)
+    fields = [f for f, _ in py._fields_]
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ap26.h"', "int main(void) {",
+             f'  printf("%zu\\n", sizeof({cname}));']
+    lines += [f'  printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([cc, "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert out[0] == ctypes.sizeof(py), (cname, out[0], ctypes.sizeof(py))
+    assert out[1:] == [getattr(py, f).offset for f in fields], cname
