@@ -2,7 +2,7 @@
  * product code: nothing in ap26_b200/ links, loads or calls it.
  *
  * A second CPU restatement of the per-K search (ibethune/ap26), written for
- * AVX-512 (F/VL/BW + VBMI2) where the reference stops at AVX2
+ * AVX-512 (F/VL/BW/DQ + VBMI2) where the reference stops at AVX2
  * (src/cpu/cpuavx2.cpp).  Same results as the plain oracle (ap26_oracle.c):
  * the candidate set of a lattice range, and the raw reports with the
  * candidate each comes from.  Two changes of method, both exact:
@@ -10,12 +10,16 @@
  *   sieve  Instead of one OKOK_{p,w} table per prime and shift word
  *          (cpusse2.cpp:38-43, sieve.cl:28-113), bit i of the 640-bit
  *          mask of all 10 words is B_p[s + i] with s = n59 * MOD^-1 mod p and
- *          B_p[j] = OK_p[((j + SHIFT) * MOD) mod p], a p-periodic bitstring
- *          (one ~2.5 KB table set per K and SHIFT).  The ten 64-bit window
- *          words of a prime are two unaligned vector loads each and one
- *          VPSHRDVQ (concatenate-and-shift) per 8 words, ANDed into the
- *          mask; primes run in ascending order and stop when all ten words
- *          are zero.
+ *          B_p[j] = OK_p[((j + SHIFT) * MOD) mod p], a p-periodic bitstring.
+ *          61 and 67 share one string of period 61*67 (bit j = B_61[j] &
+ *          B_67[j]), as do 71 and 73: 81 strings for the 83 primes, about
+ *          12 KB per K and SHIFT.  The ten 64-bit window words of a string
+ *          are two unaligned vector loads each and one VPSHRDVQ
+ *          (concatenate-and-shift) per 8 words, ANDed into the mask; the
+ *          strings run in ascending order and stop when all ten words are
+ *          zero.  The window starts of a lattice value are computed for 8
+ *          strings at a time in double precision (exact below 2^53) and
+ *          advanced with the n59 step as 16-lane integer adds.
  *   chain  The base-2 strong-PRP walk of cpuavx2.cpp:532-552 with a 64-bit
  *          Montgomery product (REDC, R = 2^64, N < 2^62) instead of the x87
  *          quotient estimate of PrimeQ_x86.h:114-136; same verdicts.
@@ -38,36 +42,42 @@ uint64_t ao_avx2_order_key(uint64_t pos);
 #define NPR 83
 #define NUM_N43 10840
 #define PER_N43 443555
-#define TGT __attribute__((target("avx512f,avx512vl,avx512bw,avx512vbmi2")))
+#define TGT __attribute__((target("avx512f,avx512vl,avx512bw,avx512dq,avx512vbmi2")))
 
 int a5_supported(void) {
   __builtin_cpu_init();
   return __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512vl") &&
-         __builtin_cpu_supports("avx512bw") && __builtin_cpu_supports("avx512vbmi2");
+         __builtin_cpu_supports("avx512bw") && __builtin_cpu_supports("avx512dq") &&
+         __builtin_cpu_supports("avx512vbmi2");
 }
 
 /* ---- per-(K, SHIFT) tables ------------------------------------------------ */
+/* Sieve units: the pair strings of 61*67 and 71*73 (bit t = B_p[t] & B_q[t],
+ * period p*q; a lattice value's window starts at n59 * MOD^-1 mod p*q,
+ * whose residues mod p and q are the two primes' own starts), then primes
+ * 79..541 one string each: 81 units for the 83 primes. */
+#define NU 81
+#define NUV 96                       /* padded to 6 vectors of 16 lanes */
 typedef struct {
-  int p[NPR];
-  double invp[NPR];
-  uint64_t *tab[NPR];          /* bit t = B_p[t mod p], NW words                 */
-  int minv[NPR];               /* MOD^-1 mod p                                    */
-  uint32_t pv[96], dv[96];     /* p and S59 * MOD^-1 mod p, padded to 6 x 16 lanes */
-  uint32_t dw[96];             /* (S59 - MOD) * MOD^-1 = dv - 1 mod p: a step that wraps */
-  int64_t s[9];                /* STEP, n0, S31, S37, S41, S43, S47, S53, S59      */
+  uint32_t P[NUV];                   /* unit period                                */
+  uint32_t minv[NUV];                /* MOD^-1 mod P                               */
+  uint32_t dv[NUV], dw[NUV];         /* S59 * MOD^-1 mod P, and that minus 1 (wrap) */
+  uint32_t off[NUV];                 /* the unit's first word in tabs               */
+  double invP[NUV];
+  uint64_t *tabs;                    /* all units' strings, bit t = unit bit t mod P */
+  int64_t s[9];                      /* STEP, n0, S31, S37, S41, S43, S47, S53, S59 */
   int64_t n43[NUM_N43];
   int shift;
 } a5_k;
 
-static int inv_mod(int a, int p) {            /* a^(p-2) mod p */
-  int r = 1, e = p - 2;
-  a %= p;
-  while (e) {
-    if (e & 1) r = r * a % p;
-    a = a * a % p;
-    e >>= 1;
+static int inv_mod(int a, int p) {   /* a^-1 mod p by the extended Euclid */
+  int t = 0, nt = 1, r = p, nr = ((a % p) + p) % p;
+  while (nr) {
+    int q = r / nr, x = t - q * nt;
+    t = nt; nt = x;
+    x = r - q * nr; r = nr; nr = x;
   }
-  return r;
+  return t < 0 ? t + p : t;
 }
 
 static a5_k *a5_build(int K, int shift) {
@@ -75,30 +85,50 @@ static a5_k *a5_build(int K, int shift) {
   ao_setup(K, k->s);
   ao_n43(K, k->n43);
   k->shift = shift;
-  uint8_t ok[541];
+  static const int pair[2][2] = {{61, 67}, {71, 73}};
+  uint8_t ok[NPR][541];
+  int pr[NPR];
   for (int i = 0; i < NPR; i++) {
-    const int p = ao_prime(i);
-    k->p[i] = p;
-    k->invp[i] = 1.0 / p;
-    ao_ok_table(K, p, ok);
-    const int mp = (int)(MOD % p);
-    const int nw = (p - 1) / 64 + 12;   /* window words up to (s >> 6) + 10 */
-    k->tab[i] = calloc(nw, sizeof(uint64_t));
-    for (int t = 0; t < nw * 64; t++) {
-      const int j = t % p;
-      if (ok[(int)(((int64_t)(j + shift % p) * mp) % p)]) k->tab[i][t >> 6] |= 1ull << (t & 63);
-    }
-    k->minv[i] = inv_mod(mp, p);
-    k->pv[i] = (uint32_t)p;
-    k->dv[i] = (uint32_t)((k->s[8] % p) * k->minv[i] % p);
-    k->dw[i] = (k->dv[i] + (uint32_t)p - 1) % (uint32_t)p;
+    pr[i] = ao_prime(i);
+    ao_ok_table(K, pr[i], ok[i]);
   }
-  for (int i = NPR; i < 96; i++) { k->pv[i] = 1; k->dv[i] = 0; k->dw[i] = 0; }
+  uint32_t total = 0;
+  for (int u = 0; u < NU; u++) {
+    const int P = u < 2 ? pair[u][0] * pair[u][1] : pr[u + 2];
+    k->P[u] = (uint32_t)P;
+    k->off[u] = total;
+    total += (uint32_t)((P - 1) / 64 + 12);   /* window words up to (s >> 6) + 10 */
+  }
+  k->tabs = calloc(total, sizeof(uint64_t));
+  for (int u = 0; u < NU; u++) {
+    const int P = (int)k->P[u];
+    const int np = u < 2 ? 2 : 1;
+    const int ps[2] = {u < 2 ? pair[u][0] : P, u < 2 ? pair[u][1] : P};
+    const int nw = (P - 1) / 64 + 12;
+    uint64_t *tab = k->tabs + k->off[u];
+    for (int t = 0; t < nw * 64; t++) {
+      int on = 1;
+      for (int q = 0; q < np && on; q++) {
+        const int p = ps[q], gi = u < 2 ? 2 * u + q : u + 2;
+        const int mp = (int)(MOD % p), j = t % p;
+        on = ok[gi][(int)(((int64_t)(j + shift % p) * mp) % p)];
+      }
+      if (on) tab[t >> 6] |= 1ull << (t & 63);
+    }
+    const int mP = (int)(MOD % P);
+    k->minv[u] = (uint32_t)inv_mod(mP, P);
+    k->invP[u] = 1.0 / P;
+    k->dv[u] = (uint32_t)((int64_t)(k->s[8] % P) * k->minv[u] % P);
+    k->dw[u] = (k->dv[u] + (uint32_t)P - 1) % (uint32_t)P;
+  }
+  for (int u = NU; u < NUV; u++) {
+    k->P[u] = 1; k->minv[u] = 0; k->dv[u] = 0; k->dw[u] = 0; k->off[u] = 0; k->invP[u] = 1.0;
+  }
   return k;
 }
 
 static void a5_free(a5_k *k) {
-  for (int i = 0; i < NPR; i++) free(k->tab[i]);
+  free(k->tabs);
   free(k);
 }
 
@@ -117,53 +147,72 @@ static int64_t n59_of(const a5_k *k, int64_t f) {
   return v;
 }
 
-static inline int mod_p(int64_t x, int p, double inv) {     /* 0 <= x < 2^53 */
-  int64_t q = (int64_t)((double)x * inv);
-  int64_t r = x - q * p;
-  if (r < 0) r += p;
-  else if (r >= p) r -= p;
-  return (int)r;
+/* x mod P for 8 lanes of doubles holding integers below 2^53: the quotient
+ * estimate floor(x / P) is off by at most one, so one correction each way. */
+TGT static inline __m512d mod_pd(__m512d x, __m512d P, __m512d iP) {
+  const __m512d q = _mm512_roundscale_pd(_mm512_mul_pd(x, iP),
+                                         _MM_FROUND_TO_NEG_INF | _MM_FROUND_NO_EXC);
+  __m512d r = _mm512_fnmadd_pd(q, P, x);
+  r = _mm512_mask_add_pd(r, _mm512_cmp_pd_mask(r, _mm512_setzero_pd(), _CMP_LT_OQ), r, P);
+  r = _mm512_mask_sub_pd(r, _mm512_cmp_pd_mask(r, P, _CMP_GE_OQ), r, P);
+  return r;
 }
 
-/* Window starts s_p = n59 * MOD^-1 mod p of all primes (st[0..82]). */
-static void starts_of(const a5_k *k, int64_t n59, uint32_t *st) {
-  for (int i = 0; i < NPR; i++) {
-    const int r = mod_p(n59, k->p[i], k->invp[i]);
-    st[i] = (uint32_t)mod_p((int64_t)r * k->minv[i], k->p[i], k->invp[i]);
+/* Window starts s_u = n59 * MOD^-1 mod P_u of all units (n59 < 2^48). */
+TGT static void starts_of(const a5_k *k, int64_t n59, uint32_t *st) {
+  const __m512d x = _mm512_set1_pd((double)n59);
+  for (int v = 0; v < NUV; v += 8) {
+    const __m512d P = _mm512_cvtepu32_pd(_mm256_loadu_si256((const __m256i *)(k->P + v)));
+    const __m512d iP = _mm512_loadu_pd(k->invP + v);
+    const __m512d mi = _mm512_cvtepu32_pd(_mm256_loadu_si256((const __m256i *)(k->minv + v)));
+    const __m512d r = mod_pd(x, P, iP);                       /* n59 mod P */
+    const __m512d s = mod_pd(_mm512_mul_pd(r, mi), P, iP);    /* < 2^25 before the mod */
+    _mm256_storeu_si256((__m256i *)(st + v), _mm512_cvttpd_epu32(s));
   }
-  for (int i = NPR; i < 96; i++) st[i] = 0;
 }
 
-/* n59 -> n59 + S59 (mod MOD): every start advances by S59 * MOD^-1 mod p,
- * and by one less when the sum wrapped (MOD is not 0 mod p). */
+/* n59 -> n59 + S59 (mod MOD): every start advances by S59 * MOD^-1 mod P,
+ * and by one less when the sum wrapped (MOD is not 0 mod P). */
 TGT static void advance_starts(const a5_k *k, uint32_t *st, int wrapped) {
   const uint32_t *d = wrapped ? k->dw : k->dv;
-  for (int v = 0; v < 96; v += 16) {
+  for (int v = 0; v < NUV; v += 16) {
     __m512i x = _mm512_add_epi32(_mm512_loadu_si512(st + v), _mm512_loadu_si512(d + v));
-    x = _mm512_min_epu32(x, _mm512_sub_epi32(x, _mm512_loadu_si512(k->pv + v)));
+    x = _mm512_min_epu32(x, _mm512_sub_epi32(x, _mm512_loadu_si512(k->P + v)));
     _mm512_storeu_si512(st + v, x);
   }
 }
 
-/* The sieved 640-bit mask of n59 (window starts st): m[0..9] = words 0..9.
- * All ten words in every step (8 + 2 lanes); the mask is tested for zero
- * every fourth prime.  (A scalar per-word tail after 12-24 vector primes,
- * as the GPU kernel does, measured 1.3-2.7x slower here: the branch on each
- * word's death mispredicts.) */
-TGT static void sieve_n59(const a5_k *k, const uint32_t *st, uint64_t m[10]) {
+/* First table word of each unit's window: off_u + s_u / 64. */
+TGT static void window_words(const a5_k *k, const uint32_t *st, uint32_t *idx) {
+  for (int v = 0; v < NUV; v += 16)
+    _mm512_storeu_si512(idx + v, _mm512_add_epi32(_mm512_loadu_si512(k->off + v),
+                                                  _mm512_srli_epi32(_mm512_loadu_si512(st + v), 6)));
+}
+
+/* The sieved 640-bit mask of n59 (window starts st, first words idx):
+ * m[0..9] = words 0..9.  All ten words in every step (8 + 2 lanes).  The
+ * first 20 units run unconditionally (the mask of under 1% of lattice
+ * values dies before unit 20) and the mask is then tested for zero every
+ * second unit, in one test of the OR of both parts.  (A scalar per-word
+ * tail after 12-24 vector primes, as the GPU kernel does, measured
+ * 1.3-2.7x slower here: the branch on each word's death mispredicts.)  The
+ * shift of a window is broadcast as a 32-bit value: VPSHRDVQ reads the low
+ * 6 bits of each 64-bit count, s mod 64. */
+TGT static void sieve_n59(const a5_k *k, const uint32_t *st, const uint32_t *idx, uint64_t m[10]) {
   __m512i acc8 = _mm512_set1_epi64(-1);
   __m128i acc2 = _mm_set1_epi64x(-1);
-  for (int i = 0; i < NPR; i++) {
-    const int s = (int)st[i];
-    const uint64_t *t = k->tab[i] + (s >> 6);
-    const __m512i sh8 = _mm512_set1_epi64(s & 63);
+  const uint64_t *tabs = k->tabs;
+  for (int u = 0; u < NU; u++) {
+    const uint64_t *t = tabs + idx[u];
+    const __m512i sh = _mm512_set1_epi32((int)st[u]);
     acc8 = _mm512_and_si512(acc8, _mm512_shrdv_epi64(_mm512_loadu_si512(t),
-                                                     _mm512_loadu_si512(t + 1), sh8));
+                                                     _mm512_loadu_si512(t + 1), sh));
     acc2 = _mm_and_si128(acc2, _mm_shrdv_epi64(_mm_loadu_si128((const __m128i *)(t + 8)),
                                                _mm_loadu_si128((const __m128i *)(t + 9)),
-                                               _mm512_castsi512_si128(sh8)));
-    if ((i & 3) == 3 && !_mm512_test_epi64_mask(acc8, acc8) &&
-        !_mm_test_epi64_mask(acc2, acc2))
+                                               _mm512_castsi512_si128(sh)));
+    if (u >= 19 && (u & 1) == 1 &&
+        !_mm512_test_epi64_mask(_mm512_or_si512(acc8, _mm512_zextsi128_si512(acc2)),
+                                _mm512_or_si512(acc8, _mm512_zextsi128_si512(acc2))))
       break;
   }
   _mm512_storeu_si512(m, acc8);
@@ -234,7 +283,8 @@ static void *worker(void *arg) {
   a5_job *J = (a5_job *)arg;
   const a5_k *k = J->k;
   uint64_t m[10];
-  uint32_t st[96] __attribute__((aligned(64)));
+  uint32_t st[NUV] __attribute__((aligned(64)));
+  uint32_t idx[NUV] __attribute__((aligned(64)));
   int64_t n59 = 0;
   for (int64_t f = J->f0; f < J->f1; f++) {
     if (f == J->f0 || f % 35 == 0) {        /* new n53: starts from scratch */
@@ -246,7 +296,8 @@ static void *worker(void *arg) {
       if (wrapped) n59 -= MOD;
       advance_starts(k, st, wrapped);
     }
-    sieve_n59(k, st, m);
+    window_words(k, st, idx);
+    sieve_n59(k, st, idx, m);
     for (int w = 0; w < 10; w++) {
       uint64_t bits = m[w];
       while (bits) {
