@@ -27,10 +27,12 @@
 // into ONE window of a p-periodic bitstring:
 //     B_p[j] = OK_p[((j + SHIFT) * MOD) mod p],
 //     bit i of the 640-bit mask = B_p[s + i],  s = n59 * MOD^-1 mod p.
-// So each prime needs a (p + 672)-bit string (10.7 KB in all, kept in
-// shared memory) and, per n59, one window offset.  Reading the window is
+// So each prime needs a (p + 672)-bit string and, per n59, one window
+// offset: 2806 words (11.2 KB) per (K, SHIFT) with the pair strings below,
+// staged in shared memory per CTA (the dense primes' words as overlapping
+// 128-bit quads, the rest once: 20.8 KB for G = 22).  Reading a window is
 // conflict-free: all lanes read the same prime's string at word offsets
-// that differ by at most (p-1)/32 < 17, i.e. inside one 32-bank row.
+// that differ by at most (p-1)/32 < 17, within one 32-bank row.
 // Primes 61 and 67 share one string of period 4087 (bit j = B_61[j] &
 // B_67[j], window start n59 * MOD^-1 mod 4087), and 71 and 73 one of
 // period 5183; their windows are read conflict-free because the starts of
@@ -38,8 +40,8 @@
 // so a warp's 32 starts lie close together in both strings.
 //
 //   dense phase  the first G primes for all 10 words of every n59: G-2
-//                windows (the two pairs, primes 4..G-1), each 21 word loads
-//                + 20 funnel shifts
+//                windows (the two pairs, primes 4..G-1), each five 128-bit
+//                loads and one 32-bit load + 20 funnel shifts
 //   tail         live (n59, word) pairs are compacted into a per-warp shared
 //                queue (ballot/popc) and advanced R primes at a time, all
 //                lanes on the same prime, until stage SL

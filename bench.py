@@ -790,7 +790,7 @@ def main():
                        "kmin": KMIN_SEEDED, "k_per_rank": RANGE_K, "shift": SHIFT,
                        "searched_k": int(ks_total), "raw_k": int(raw_total),
                        "parallelism": f"replicas x{world} (disjoint K ranges)",
-                       "l2": "working set is a 10 KB table per K in shared memory; no "
+                       "l2": "working set is an 11 KB table per K in shared memory; no "
                              "HBM-resident inputs to flush",
                        "autotuned": tuned},
             "raw_kps": raw_total / (dev_ms / 1000.0),
