@@ -269,8 +269,10 @@ def item_parity(A, items, got_reports, got_hashes):
         ks += sum(will_search(K) for K in range(a, b + 1))
         if [tuple(r[:3]) for r in reps] != exp or h != host_hash(A, exp):
             bad.append(iid)
+    # no item checked is no parity claim: ok needs at least one checked item
     return {"items_checked_vs_reference": checked, "k_checked": ks, "items": len(items),
-            "all_items_checked": checked == len(items), "mismatched": bad, "ok": not bad}
+            "all_items_checked": checked == len(items), "mismatched": bad,
+            "ok": checked > 0 and not bad}
 
 
 def parity_check(seen, kmin):
@@ -286,7 +288,7 @@ def parity_check(seen, kmin):
         if seen[K] != ref:
             bad.append(K)
     return {"k_checked_vs_reference": checked, "k_with_reports": len(seen),
-            "mismatched": bad, "ok": not bad}
+            "mismatched": bad, "ok": checked > 0 and not bad}
 
 
 # ---- reference arm ---------------------------------------------------------------
