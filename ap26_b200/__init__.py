@@ -39,7 +39,7 @@ class Opts(ctypes.Structure):
                 ("chunk_tiles", ctypes.c_int32), ("use_graphs", ctypes.c_int32),
                 ("profile", ctypes.c_int32), ("cand_ring_log2", ctypes.c_int32),
                 ("mem_budget", ctypes.c_int64), ("wait_timeout_s", ctypes.c_double),
-                ("tail_group", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("tail_group", ctypes.c_int32), ("batch_wave", ctypes.c_int32)]
 
 
 class AP(ctypes.Structure):

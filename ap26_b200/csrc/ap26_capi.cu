@@ -550,6 +550,12 @@ extern "C" const char *ap26_last_error(const ap26_ctx *ctx) {
   return ctx ? ctx->last_error.c_str() : "";
 }
 
+// K-jobs per run of ap26_search_batch (ap26_opts.batch_wave): by default
+// about 3 minutes of device time and at most a few hundred thousand raw
+// reports (the main set holds 2^20); at most 2048 (about 12 minutes).
+constexpr int kBatchWave = 512;
+constexpr int kMaxBatchWave = 2048;
+
 static int default_opts(ap26_opts *o) {
   if (!o->dense_primes) o->dense_primes = kVariants[0].G;
   if (!o->warp_queue) o->warp_queue = kVariants[0].QCAP;
@@ -560,6 +566,7 @@ static int default_opts(ap26_opts *o) {
   if (!o->use_graphs) o->use_graphs = 1;
   if (!o->cand_ring_log2) o->cand_ring_log2 = 26;
   if (!(o->wait_timeout_s > 0)) o->wait_timeout_s = 3600.0;
+  if (o->batch_wave <= 0) o->batch_wave = kBatchWave;
   return 0;
 }
 
@@ -701,7 +708,8 @@ extern "C" int ap26_create(int device, const ap26_opts *opts, ap26_ctx **out) {
     CKC(cudaFuncSetAttribute(admit_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)ORDER_SMEM));
     // buffers
-    if (ctx->opts.cand_ring_log2 < 12 || ctx->opts.cand_ring_log2 > 27) {
+    if (ctx->opts.cand_ring_log2 < 12 || ctx->opts.cand_ring_log2 > 27 ||
+        ctx->opts.batch_wave > kMaxBatchWave) {
       rc = AP26_E_ARG;
       goto fail;
     }
@@ -781,9 +789,11 @@ extern "C" int ap26_set_opts(ap26_ctx *ctx, const ap26_opts *opts) {
   if (opts->cand_ring_log2) o.cand_ring_log2 = opts->cand_ring_log2;
   if (opts->wait_timeout_s > 0) o.wait_timeout_s = opts->wait_timeout_s;
   if (opts->use_graphs) o.use_graphs = opts->use_graphs;
+  if (opts->batch_wave) o.batch_wave = opts->batch_wave;
   o.profile = opts->profile;
   const int vi = pick_variant(o);
-  if (vi < 0 || o.cand_ring_log2 < 12 || o.cand_ring_log2 > 27 || o.chunk_tiles < 1)
+  if (vi < 0 || o.cand_ring_log2 < 12 || o.cand_ring_log2 > 27 || o.chunk_tiles < 1 ||
+      o.batch_wave < 1 || o.batch_wave > kMaxBatchWave)
     return AP26_E_ARG;
   if (o.mem_budget != ctx->opts.mem_budget && ctx->d_pool) return AP26_E_ARG;
   if (!serving_idle(ctx)) return AP26_E_ARG;   // slices in flight use the rings
@@ -1251,6 +1261,21 @@ extern "C" int ap26_search_k_sol(ap26_ctx *ctx, int K, int shift, int iter,
 }
 
 // ---- batched persistent form ------------------------------------------------------
+// Sums the stats of consecutive runs of one call.
+static void add_stats(ap26_stats &a, const ap26_stats &b) {
+  a.candidates += b.candidates;
+  a.late_items += b.late_items;
+  a.prp_tests += b.prp_tests;
+  a.aps += b.aps;
+  a.device_ms += b.device_ms;
+  a.error_flags |= b.error_flags;
+  a.launches += b.launches;
+  a.sieve_ms += b.sieve_ms;
+  a.sieve_cells += b.sieve_cells;
+  a.sieve_launches += b.sieve_launches;
+  a.chain_walks += b.chain_walks;
+}
+
 extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
                                  ap26_ap *aps, int64_t ap_cap, int64_t *n_aps,
                                  ap26_item_result *res, ap26_stats *stats) {
@@ -1265,25 +1290,38 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
     for (int K = it.kmin; K <= it.kmax; K++)
       if (ap26_will_search(K)) jobs.push_back({i, K});
   }
-  int rc;
-  if ((rc = jobset_ensure(ctx, ctx->main, (int)jobs.size())) != AP26_OK) return rc;
-  for (size_t j = 0; j < jobs.size(); j++)
-    fill_job(ctx->main.h_jobs[j], jobs[j].second, items[jobs[j].first].shift, jobs[j].first, 0,
-             N53_PER_K);
-  long long n = 0;
-  if (!jobs.empty()) {
-    rc = run_jobs_retry(ctx, (int)jobs.size(), false, stats, &n, true);
-    if (rc != AP26_OK) return rc;
-  } else if (stats) {
-    memset(stats, 0, sizeof(*stats));
-  }
-  const JobSet &S = ctx->main;
-  // group reports: item, K ascending, AVX2 order inside K
+  // the K-jobs run in waves of at most opts.batch_wave: the report buffer
+  // and each device wait stay bounded whatever the batch's size
   std::vector<std::vector<RepOut>> per_item(n_items);
-  for (auto &r : collect_reports(S, n)) per_item[S.h_jobs[r.first].item].push_back(r.second);
-  int64_t total = 0;
   std::vector<unsigned long long> hash_add(n_items, 0);
-  for (size_t j = 0; j < jobs.size(); j++) hash_add[jobs[j].first] += job_hash_total(S, (int)j);
+  std::vector<int64_t> cand(n_items, 0);
+  std::vector<int32_t> nks(n_items, 0);
+  if (stats) memset(stats, 0, sizeof(*stats));
+  const JobSet &S = ctx->main;
+  const size_t wave = (size_t)ctx->opts.batch_wave;
+  for (size_t w0 = 0; w0 < jobs.size(); w0 += wave) {
+    const int nw = (int)std::min(wave, jobs.size() - w0);
+    int rc;
+    if ((rc = jobset_ensure(ctx, ctx->main, nw)) != AP26_OK) return rc;
+    for (int j = 0; j < nw; j++) {
+      const auto &jb = jobs[w0 + j];
+      fill_job(ctx->main.h_jobs[j], jb.second, items[jb.first].shift, jb.first, 0, N53_PER_K);
+    }
+    long long n = 0;
+    ap26_stats st;
+    rc = run_jobs_retry(ctx, nw, false, stats ? &st : nullptr, &n, true);
+    if (rc != AP26_OK) return rc;
+    // reports grouped by item here, put in K and AVX2 order below
+    for (auto &r : collect_reports(S, n)) per_item[S.h_jobs[r.first].item].push_back(r.second);
+    for (int j = 0; j < nw; j++) {
+      const int item = S.h_jobs[j].item;
+      hash_add[item] += job_hash_total(S, j);
+      cand[item] += (int64_t)S.h_job_counts[j];
+      nks[item]++;
+    }
+    if (stats) add_stats(*stats, st);
+  }
+  int64_t total = 0;
   for (int i = 0; i < n_items; i++) {
     auto &v = per_item[i];
     std::sort(v.begin(), v.end(), rep_less);
@@ -1293,15 +1331,11 @@ extern "C" int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_it
       if (r.fin.status != AP26_OK) { res[i].status = r.fin.status; break; }
     res[i].n_aps = (int32_t)v.size();
     res[i].first_ap = total;
-    res[i].candidates = 0;
-    res[i].ks_searched = 0;
+    res[i].candidates = cand[i];
+    res[i].ks_searched = nks[i];
     res[i].result_hash = hash_fold(0, hash_add[i]);
     res[i].latency_ms = 0;
     total += (int64_t)v.size();
-  }
-  for (size_t j = 0; j < jobs.size(); j++) {
-    res[jobs[j].first].candidates += (int64_t)S.h_job_counts[j];
-    res[jobs[j].first].ks_searched++;
   }
   *n_aps = total;
   if (total > ap_cap) return AP26_E_CAPACITY;
@@ -1705,15 +1739,21 @@ extern "C" int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int sh
   if (!ctx || !Ks || nK <= 0 || !counts) return AP26_E_ARG;
   CK(cudaSetDevice(ctx->device));
   drain(ctx);
-  int rc;
-  if ((rc = jobset_ensure(ctx, ctx->main, nK)) != AP26_OK) return rc;
-  for (int i = 0; i < nK; i++) {
+  for (int i = 0; i < nK; i++)
     if (!k_in_domain(Ks[i], shift)) return AP26_E_DOMAIN;
-    fill_job(ctx->main.h_jobs[i], Ks[i], shift, i, 0, N53_PER_K);
+  if (stats) memset(stats, 0, sizeof(*stats));
+  // waves of at most opts.batch_wave K, as ap26_search_batch
+  for (int w0 = 0; w0 < nK; w0 += ctx->opts.batch_wave) {
+    const int nw = std::min(ctx->opts.batch_wave, nK - w0);
+    int rc;
+    if ((rc = jobset_ensure(ctx, ctx->main, nw)) != AP26_OK) return rc;
+    for (int i = 0; i < nw; i++) fill_job(ctx->main.h_jobs[i], Ks[w0 + i], shift, i, 0, N53_PER_K);
+    ap26_stats st;
+    rc = run_jobs(ctx, nw, true, stats ? &st : nullptr, nullptr);
+    if (rc != AP26_OK) return rc;
+    for (int i = 0; i < nw; i++) counts[w0 + i] = (int64_t)ctx->main.h_job_counts[i];
+    if (stats) add_stats(*stats, st);
   }
-  rc = run_jobs(ctx, nK, true, stats, nullptr);
-  if (rc != AP26_OK) return rc;
-  for (int i = 0; i < nK; i++) counts[i] = (int64_t)ctx->main.h_job_counts[i];
   return AP26_OK;
 }
 

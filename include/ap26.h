@@ -81,7 +81,10 @@ typedef struct {
                              first waits for the abandoned work to finish     */
   int32_t tail_group;     /* primes a queued shift word advances per pass of
                              the tail stages                                  */
-  int32_t reserved;
+  int32_t batch_wave;     /* K-jobs per run of ap26_search_batch (default 512,
+                             1..2048): a batch of any size runs as waves of
+                             this many, so the report buffer and each device
+                             wait stay bounded                                */
 } ap26_opts;
 
 /* One raw report: AP length k, difference multiplier K, first term, and the
@@ -225,10 +228,13 @@ int ap26_search_k_sol_words(ap26_ctx *ctx, int K, int shift, int iter, int32_t *
 /* ---- batched persistent form ----------------------------------------------
  * All searchable K of all items in one persistent work-stealing pipeline:
  * sieve tiles of every item share launches, survivors of every K share PRP
- * batches, and the whole run (set-up, chunks, chain walks, ReportSolution,
- * read-backs) is one CUDA-graph launch (ap26_opts.use_graphs).  Reports are grouped per item (res[i].first_ap, res[i].n_aps),
- * inside an item by K ascending, inside a K in AVX2 order.  No counterpart
- * in the reference: it replaces the per-K loop of AP26.cpp:957-982 when many
+ * batches, and each run (set-up, chunks, chain walks, ReportSolution,
+ * read-backs) is one CUDA-graph launch (ap26_opts.use_graphs).  A batch of
+ * more than ap26_opts.batch_wave K-jobs runs as consecutive runs of that
+ * many, so any batch size fits the report buffer and the wait limit.
+ * Reports are grouped per item (res[i].first_ap, res[i].n_aps), inside an
+ * item by K ascending, inside a K in AVX2 order.  No counterpart in the
+ * reference: it replaces the per-K loop of AP26.cpp:957-982 when many
  * workunits run in one process. */
 int ap26_search_batch(ap26_ctx *ctx, const ap26_item *items, int n_items,
                       ap26_ap *aps, int64_t ap_cap, int64_t *n_aps,
@@ -285,7 +291,8 @@ int ap26_serve_memory(const ap26_ctx *ctx, int64_t *in_use, int64_t *budget);
 int ap26_sieve_range(ap26_ctx *ctx, int K, int shift, int64_t q_begin,
                      int64_t q_end, int64_t *cand, int64_t cap,
                      int64_t *n_cand, ap26_stats *stats);
-/* Sieve survivor counts for nK values of K at one SHIFT (counts only). */
+/* Sieve survivor counts for nK values of K at one SHIFT (counts only), in
+ * runs of at most ap26_opts.batch_wave K. */
 int ap26_sieve_count(ap26_ctx *ctx, const int32_t *Ks, int nK, int shift,
                      int64_t *counts, ap26_stats *stats);
 /* Base-2 strong-PRP verdicts (1 = probable prime) for odd N in (2, 2^63).

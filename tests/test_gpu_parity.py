@@ -257,6 +257,27 @@ def test_batch_equals_plain(ctx):
         assert r.result_hash == rep.hash.value   # device-side ReportSolution
 
 
+def test_batch_in_waves_equals_one_run():
+    """A batch runs as waves of opts.batch_wave K-jobs (the report buffer
+    and each device wait stay bounded for any batch): waves of 2 give each
+    item the reports, hash, candidates and K count of a single run."""
+    items = [(7, 366384, 366384, 0), (8, 1000037, 1000040, 640), (9, 2000003, 2000003, 1280),
+             (10, 58 * 59, 58 * 59, 0)]
+    with A.Context(0) as c:
+        per1, res1, st1 = c.search_batch(items)
+    with A.Context(0, batch_wave=2) as c:
+        assert c.opts["batch_wave"] == 2
+        per2, res2, st2 = c.search_batch(items)
+    assert per2 == per1
+    for a, b in zip(res1, res2):
+        assert (a.id, a.status, a.n_aps, a.candidates, a.ks_searched, a.result_hash) == \
+            (b.id, b.status, b.n_aps, b.candidates, b.ks_searched, b.result_hash)
+    assert st2.candidates == st1.candidates == st2.chain_walks
+    assert st2.aps == st1.aps
+    with pytest.raises(A.AP26Error):
+        A.Context(0, batch_wave=4096)
+
+
 def test_serving_alone_equals_mixed(ctx):
     units = [(1, 3000017, 3000019, 0), (2, 4000037, 4000037, 640), (3, 5000011, 5000013, 1280)]
     alone = {}
