@@ -68,8 +68,10 @@ constexpr int TABLE_WORDS = word_offset(NPRIMES);   // 2806 words, 11224 bytes
 // (at most 3), and k2 likewise mod 5183.  Starts are ordered by k1 in
 // buckets of ORDER_BUCKET values, and by k2 inside a bucket (about 320
 // starts each).  The 32 starts of a warp then lie within about 230 bits of
-// each other in the first string and 870 bits in the second, a half warp
-// within half that, so neither pair bitstring's 64-bit loads conflict.  The
+// each other in the first string and 870 bits in the second, and the 8
+// starts of a quarter warp (one phase of a 128-bit load) nearly always
+// within 8 consecutive quad entries: a CPU model of the order counts no
+// extra wavefronts for the first string and 1-3% for the second.  The
 // order is one 16-bit index per start, built with the tables.
 constexpr int ORDER_BUCKET = 103;
 constexpr int PERM_WORDS = (N53_PER_N43 + 1) / 2;   // 6337 words
