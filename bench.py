@@ -346,7 +346,7 @@ BATCHED_MAX_LEN = 64           # ... of log-uniform length 1..64 K
 BATCHED_ITEMS = 5              # bench prefix: the first 5 items (20 searchable K)
 SERVE_UNITS, SERVE_MAX_K = 32, 8
 SIEVE_PAIR_KMIN = 27872096     # default_rng(31).integers(1e6, 5e7 - 1024): 1024 K at SHIFT 640
-SIEVE_PAIR_FULL, SIEVE_PAIR_K, SIEVE_PAIR_PINNED, SIEVE_PAIR_SHIFT = 1024, 64, 16, 640
+SIEVE_PAIR_FULL, SIEVE_PAIR_K, SIEVE_PAIR_PINNED, SIEVE_PAIR_SHIFT = 1024, 64, 56, 640
 
 
 def batched_items(n=BATCHED_ITEMS):
@@ -368,7 +368,7 @@ def sieve_pair_ks(n=SIEVE_PAIR_K):
 
 def fixture_pairs():
     """Every (K, SHIFT) of the secondary workloads whose reference results are
-    recorded: the first 16 searchable K of the sieve pair, then the batched
+    recorded: the 56 searchable K of the sieve pair's first 64, then the batched
     and serving items' searchable K."""
     out = [(k, SIEVE_PAIR_SHIFT) for k in sieve_pair_ks() if will_search(k)][:SIEVE_PAIR_PINNED]
     for _, a, b, sh in batched_items() + serve_units():
