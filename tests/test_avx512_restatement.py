@@ -30,6 +30,10 @@ def a5(oracle):
     (44121555, 640, 10 ** 9 + 17, 10 ** 9 + 400_017),  # ragged, mid-lattice
     (1, 15360, 4_808_136_200 - 300_000, 4_808_136_200),  # end of the lattice, largest SHIFT
     (400_000_000, 1280, 2_000_000_000, 2_000_250_000),   # largest K in the domain
+    # 61*67*71*73: all four primes of the two pair strings divide K, so each
+    # bans one residue instead of 24 (the densest searchable K)
+    (21182921, 640, 3_000_000_000, 3_000_300_000),
+    (61 * 67 * 30, 0, 123_456, 423_456),                # 61*67 | K (a searchable K)
 ])
 def test_a5_sieve_equals_oracle(a5, K, shift, f0, f1):
     cap = 1 << 20
