@@ -74,6 +74,8 @@ def oracle_sieve(oracle, K, shift, q0, q1, threads=4):
     (1, 0, 0, 30_000),                         # smallest K
     (2, 1280, 9_000_000, 9_013_000),
     (400_000_000, 640, 5_000_000, 5_020_000),  # largest K in the domain (AP26_KMAX_SAFE)
+    (21182921, 640, 60_000_000, 60_020_000),   # 61*67*71*73 | K: both pair strings
+    (61 * 67 * 30, 0, 3_000_000, 3_013_000),   # 61*67 | K
 ])
 def test_sieve_range_vs_oracle(ctx, oracle, K, shift, q0, q1):
     if not A.will_search(K):
