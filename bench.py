@@ -589,11 +589,12 @@ def measure_sprp(ctx, A, int_tops, log2=24):
 # ---- our arm ---------------------------------------------------------------------
 # DRAM bytes per sieve cell: dram__bytes_read.sum + dram__bytes_write.sum of a
 # 131072-tile launch (1.174e10 cells) of the default variant in one ncu
-# capture, 137.9 MB read + 138.3 MB written (three launches agree within 1%).
-# Nearly all of it is the candidate ring: about 9.5 M survivors x 16 B
-# written, and the L2's fills of the partly written sectors read back; it
-# grows with the survivors, so with the cells, and scales to any launch.
-SIEVE_DRAM_BYTES_PER_CELL = (137.9e6 + 138.3e6) / (131072 * 256 * 35 * 10)
+# capture, 137.7 MB read + 137.1 MB written (mean of three launches, which
+# agree within 1%).  Nearly all of it is the candidate ring: about 9.5 M
+# survivors x 16 B written, and the L2's fills of the partly written sectors
+# read back; it grows with the survivors, so with the cells, and scales to
+# any launch.
+SIEVE_DRAM_BYTES_PER_CELL = (137.67e6 + 137.15e6) / (131072 * 256 * 35 * 10)
 
 
 def main():
